@@ -1,0 +1,152 @@
+// Device-side data layout and helpers of the gstb engine (sm_100a).
+//
+// HBM layout of one query (all arrays owned by the engine):
+//   table  u64 [V][2^k][nd]   packed  cost << 32 | parent   (nd = D+1, or 1 unbounded)
+//                              parent: 00 seed | 01 grow (30-bit predecessor vertex)
+//                                      | 10 merge (p1 : 8 bits, d1 : 3, d2 : 3)
+//                              INF = all ones (memset 0xFF); a 64-bit atomicMin keeps
+//                              cost and parent consistent (no torn parents, unlike the
+//                              reference's separate stores at DPQ.cu:117-121).
+//   dist   u32 [V][8]          shortest distance from query group j to v
+//   dflag  u32 [ceil(V*2^k*nd/16)]  2 bits per state: in-near, in-far
+//   sflag  u32 [ceil(V*8/16)]      2 bits per distance item
+//   qbuf   u32 [4][cap]        near-in, near-out, far, far-out work lists of state ids
+//   tour   u32 [k][2^k][k] + [k][2^k]   group-tour tables P and T2 (lower bounds)
+#pragma once
+#include <cstdint>
+
+namespace gstb {
+
+constexpr uint32_t INF32 = 0xFFFFFFFFu;
+constexpr unsigned long long INF64 = 0xFFFFFFFFFFFFFFFFull;
+constexpr uint32_t BIG = 1u << 30;  // saturation value inside lower-bound sums
+constexpr uint32_t PAR_GROW = 0x40000000u;
+constexpr uint32_t PAR_MERGE = 0x80000000u;
+constexpr int KMAX = 8;
+constexpr int DMAX = 7;
+
+enum Phase : int32_t {
+  PH_IDLE = 0,
+  PH_SSSP = 1,
+  PH_DP = 2,   // unbounded DPBF
+  PH_HOP = 3,  // hop-bounded DPBF
+};
+
+// Statistics slots (match GST_STAT_* in gstb.h).
+enum {
+  ST_EXPANDED = 0,
+  ST_SSSP = 1,
+  ST_ARCS = 2,
+  ST_UPDATES = 3,
+  ST_ENQ = 4,
+  ST_ROUNDS = 5,
+  ST_MERGES = 6,
+};
+
+// Written by kernels, read back by the host after every round.
+struct alignas(16) QCtl {
+  uint32_t n_near;   // append counter of the near-out list
+  uint32_t n_far;    // append counter of the far list
+  uint32_t n_far2;   // append counter of the far-out list (split rounds)
+  uint32_t best;     // best feasible cost known (upper bound)
+  uint32_t overflow; // a list exceeded its capacity
+  uint32_t n_edges;  // extraction: number of tree edges
+  uint32_t status;   // extraction: 0 ok, 1 no solution, 2 cycle / inconsistency
+  uint32_t root;
+  unsigned long long best_full;  // min over full states of cost << 32 | payload
+  unsigned long long stat[8];
+};
+
+// Per-query descriptor; the host rewrites it before each round.
+struct QDev {
+  unsigned long long* table;
+  uint32_t* dist;
+  uint32_t* dflag;
+  uint32_t* sflag;
+  uint32_t* qbuf[4];
+  uint32_t* tour;
+  const uint32_t* members;  // distance items v*8+j of every query-group member
+  uint32_t* out_edges;      // extraction output (u, v, w) triples
+  QCtl* ctl;
+  uint32_t cap;
+  uint32_t n_members;
+  uint32_t max_edges;
+  int32_t k, D, nd, full;
+  uint32_t WT;       // 2^k * nd entries per vertex
+  int32_t phase;
+  // round fields
+  int32_t in_idx, out_idx, far_idx, far2_idx;
+  uint32_t n_in;     // items in qbuf[in_idx]
+  uint32_t n_far;    // items in qbuf[far_idx] (split input)
+  uint32_t theta_lo, theta_hi;  // current near window [lo, hi)
+  uint32_t cap1;     // distances >= cap1 are only known to be >= cap1
+};
+
+struct GraphDev {
+  const uint32_t* beg;   // [V+1]
+  const uint2* adj;      // [arcs] {neighbour, weight}, each list sorted by (weight, neighbour)
+  uint32_t V;
+};
+
+__device__ __forceinline__ unsigned long long pack(uint32_t cost, uint32_t par) {
+  return ((unsigned long long)cost << 32) | par;
+}
+
+__device__ __forceinline__ uint32_t ld_cg(const uint32_t* p) { return __ldcg(p); }
+__device__ __forceinline__ unsigned long long ld_cg(const unsigned long long* p) { return __ldcg(p); }
+
+// Software parallel-bit-deposit of the low bits of x into the set bits of mask.
+__device__ __forceinline__ uint32_t pdep(uint32_t x, uint32_t mask) {
+  uint32_t r = 0;
+  while (mask) {
+    uint32_t low = mask & (0u - mask);
+    if (x & 1u) r |= low;
+    x >>= 1;
+    mask ^= low;
+  }
+  return r;
+}
+
+__device__ __forceinline__ uint32_t sat_add(uint32_t a, uint32_t b) {
+  uint32_t s = a + b;
+  return (s < a || s > BIG) ? BIG : s;
+}
+
+// Lower bound on the cost of connecting a vertex (with group distances dl[],
+// already capped) to every group of `comp`:
+//   one-label  max_j dl_j                                   (DPQ.cu:182-188)
+//   tour lb1   min_{i,j} ceil((dl_i + P[i][comp][j] + dl_j)/2)   (CPUNONHOP.h:448-466)
+//   tour lb2   max_i ceil((dl_i + T2[i][comp] + min_j dl_j)/2)   (CPUNONHOP.h:468-472)
+// P[i][S][j] = cheapest order of visiting the groups of S starting at i and
+// ending at j with group-to-group distances as step costs; T2 = min_j P.
+__device__ __forceinline__ uint32_t lower_bound_comp(const uint32_t (&dl)[KMAX], int k,
+                                                     uint32_t comp, const uint32_t* __restrict__ P,
+                                                     const uint32_t* __restrict__ T2) {
+  if (comp == 0) return 0;
+  const uint32_t K2 = 1u << k;
+  uint32_t lb0 = 0, mind = BIG;
+#pragma unroll
+  for (int j = 0; j < KMAX; j++)
+    if (j < k && (comp >> j & 1u)) {
+      lb0 = max(lb0, dl[j]);
+      mind = min(mind, dl[j]);
+    }
+  uint32_t lb1 = BIG, lb2 = 0;
+#pragma unroll
+  for (int i = 0; i < KMAX; i++) {
+    if (i < k && (comp >> i & 1u)) {
+      const uint32_t* Pi = P + ((size_t)i * K2 + comp) * k;
+#pragma unroll
+      for (int j = 0; j < KMAX; j++)
+        if (j < k && (comp >> j & 1u)) {
+          uint32_t t = sat_add(sat_add(dl[i], __ldg(Pi + j)), dl[j]);
+          lb1 = min(lb1, (t + 1) >> 1);
+        }
+      uint32_t t2 = sat_add(sat_add(dl[i], __ldg(T2 + (size_t)i * K2 + comp)), mind);
+      lb2 = max(lb2, (t2 + 1) >> 1);
+    }
+  }
+  return max(lb0, max(lb1 >= BIG ? BIG : lb1, lb2));
+}
+
+}  // namespace gstb

@@ -1,0 +1,178 @@
+"""Python host mirror of the gstb C ABI (include/gstb.h) over ctypes.
+
+The CUDA library ``libgstb.so`` is built in-tree by ``gpugst_b200.build``.
+There is no CPU fallback: every entry point fails loudly when the library or
+a CUDA device is missing.
+
+The query surface follows the reference's: a CSR graph (beg_pos / csr /
+weight, code/GPUGST/include/graph_v_of_v_idealID/csr_graph.hpp:39-128), a
+group index (read_Group, graph_hash_of_mixed_weighted_read_for_GSTP.h:190-239),
+and per query the k group indices plus an optional hop bound D
+(DPBF_GPU, code/GPUGST/include/DPQ.cuh:63; DPBF_gpu,
+code/D-GPUGST/include/DPQ.cuh:63).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgstb.so")
+
+GST_OK, GST_NO_SOLUTION, GST_BAD_INPUT, GST_OOM = 0, 1, 2, 3
+GST_DEVICE_TIMEOUT, GST_CUDA_ERROR, GST_QUEUE_OVERFLOW, GST_TRUNCATED = 4, 5, 6, 7
+GST_INTERNAL, GST_BUSY, GST_NOT_FOUND = 8, 9, 10
+STATUS_NAMES = {0: "ok", 1: "no solution", 2: "bad input", 3: "out of memory", 4: "device timeout",
+                5: "cuda error", 6: "queue overflow", 7: "truncated", 8: "internal", 9: "busy",
+                10: "not found"}
+STAT_NAMES = ["expanded", "sssp_items", "arcs", "updates", "enqueued", "rounds", "merges", "table_bytes"]
+KMAX = 8
+
+
+class GstError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS_NAMES.get(status, status)}")
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [("cost", ctypes.c_int32), ("root", ctypes.c_uint32), ("n_edges", ctypes.c_int32),
+                ("max_edges", ctypes.c_int32), ("edges", ctypes.POINTER(ctypes.c_uint32)),
+                ("stats", ctypes.c_uint64 * 8), ("device_ms", ctypes.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libgstb.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} missing: run gpugst_b200.build.build() first")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, u32, u64, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32
+        L.gst_graph_create.argtypes = [vp, vp, vp, u32, u64, ctypes.POINTER(vp)]
+        L.gst_groups_set.argtypes = [vp, vp, vp, u32]
+        L.gst_graph_destroy.argtypes = [vp]
+        L.gst_graph_destroy.restype = None
+        L.gst_query.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Result)]
+        L.gst_query_batch.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_int]
+        L.gst_status_string.restype = ctypes.c_char_p
+        L.gst_graph_num_vertices.restype = u32
+        L.gst_graph_num_vertices.argtypes = [vp]
+        L.gst_graph_num_arcs.restype = u64
+        L.gst_graph_num_arcs.argtypes = [vp]
+        for name in ("gst_graph_create", "gst_groups_set", "gst_query", "gst_query_batch"):
+            getattr(L, name).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else None
+
+
+@dataclass
+class QueryResult:
+    status: int
+    cost: int
+    root: int
+    edges: np.ndarray  # (n, 3) uint32: u, v, w
+    stats: dict = field(default_factory=dict)
+    device_ms: float = 0.0
+
+    @property
+    def ok(self) -> bool:
+        return self.status == GST_OK
+
+
+class Engine:
+    """A graph + group index resident on the current CUDA device."""
+
+    def __init__(self, beg_pos, csr, weight, grp_ptr=None, grp_v=None):
+        L = lib()
+        self._beg = np.ascontiguousarray(beg_pos, dtype=np.uint32)
+        self._csr = np.ascontiguousarray(csr, dtype=np.uint32)
+        self._w = np.ascontiguousarray(weight, dtype=np.int32)
+        V = len(self._beg) - 1
+        h = ctypes.c_void_p()
+        st = L.gst_graph_create(_ptr(self._beg), _ptr(self._csr), _ptr(self._w), V, len(self._csr),
+                                ctypes.byref(h))
+        if st != GST_OK:
+            raise GstError(st, "gst_graph_create")
+        self._h = h
+        self.V = V
+        if grp_ptr is not None:
+            self.set_groups(grp_ptr, grp_v)
+
+    @classmethod
+    def from_instance(cls, graph, groups):
+        return cls(graph.beg_pos, graph.csr, graph.weight, groups.ptr, groups.members)
+
+    def set_groups(self, grp_ptr, grp_v):
+        self._gp = np.ascontiguousarray(grp_ptr, dtype=np.uint64)
+        self._gv = np.ascontiguousarray(grp_v, dtype=np.uint32)
+        st = lib().gst_groups_set(self._h, _ptr(self._gp), _ptr(self._gv), len(self._gp) - 1)
+        if st != GST_OK:
+            raise GstError(st, "gst_groups_set")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gst_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _unpack(st, r, buf):
+        n = min(max(r.n_edges, 0), r.max_edges)
+        edges = buf[:3 * n].reshape(-1, 3).copy() if st in (GST_OK, GST_TRUNCATED) else np.zeros((0, 3), np.uint32)
+        stats = {name: int(r.stats[i]) for i, name in enumerate(STAT_NAMES)}
+        return QueryResult(st, r.cost, r.root, edges, stats, r.device_ms)
+
+    def query(self, groups, D: int = -1, max_edges: int = 4096) -> QueryResult:
+        """One synchronous query (gst_query)."""
+        g = np.ascontiguousarray(groups, dtype=np.uint32)
+        buf = np.zeros(3 * max_edges, dtype=np.uint32)
+        r = _Result()
+        r.max_edges = max_edges
+        r.edges = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+        st = lib().gst_query(self._h, _ptr(g), len(g), int(D), ctypes.byref(r))
+        if st in (GST_CUDA_ERROR, GST_INTERNAL):
+            raise GstError(st, "gst_query")
+        return self._unpack(st, r, buf)
+
+    def query_batch(self, queries, Ds=None, max_concurrent: int = 0, max_edges: int = 4096):
+        """Many queries sharing device rounds (gst_query_batch)."""
+        n = len(queries)
+        groups = np.zeros((n, KMAX), dtype=np.uint32)
+        ks = np.zeros(n, dtype=np.int32)
+        for i, q in enumerate(queries):
+            ks[i] = len(q)
+            groups[i, :len(q)] = q
+        Darr = np.full(n, -1, dtype=np.int32) if Ds is None else np.ascontiguousarray(Ds, dtype=np.int32)
+        statuses = np.zeros(n, dtype=np.int32)
+        res = (_Result * max(n, 1))()
+        bufs = []
+        for i in range(n):
+            b = np.zeros(3 * max_edges, dtype=np.uint32)
+            bufs.append(b)
+            res[i].max_edges = max_edges
+            res[i].edges = b.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+        st = lib().gst_query_batch(self._h, n, _ptr(groups), _ptr(ks), _ptr(Darr), ctypes.cast(res, ctypes.c_void_p), _ptr(statuses),
+                                   int(max_concurrent))
+        if st != GST_OK:
+            raise GstError(st, "gst_query_batch")
+        out = [self._unpack(int(statuses[i]), res[i], bufs[i]) for i in range(n)]
+        for r in out:
+            if r.status in (GST_CUDA_ERROR, GST_INTERNAL):
+                raise GstError(r.status, "gst_query_batch")
+        return out

@@ -1,0 +1,236 @@
+"""Seeded synthetic GST instances with the shapes of the reference's datasets.
+
+The reference ships no usable dataset (its Twitch CSR blobs are missing and the
+other five live off-line), so every workload here is generated:
+
+* ``chung_lu``  -- undirected power-law graph, expected degree of vertex i
+  proportional to (i + i0)^(-1/(gamma-1)), endpoints sampled proportional to
+  that weight, self-loops and duplicate edges rejected until exactly E unique
+  edges remain.  i0 is chosen so that the largest expected degree is about
+  2*sqrt(2E) (hubs in the thousands to tens of thousands at the sizes used).
+* ``rmat``      -- R-MAT / Kronecker edges with initiator (a, b, c, d) =
+  (0.57, 0.19, 0.19, 0.05), the Graph500 values, vertex labels permuted,
+  self-loops and duplicates dropped, symmetrised.
+* ``zipf_groups`` -- group sizes ~ Zipf(s) truncated to [1, smax], members
+  uniform without replacement; every vertex left uncovered is then appended to
+  a uniformly random group, so every vertex is in at least one group.
+* ``queries``   -- k distinct group ids, uniform.
+
+Edge weights are int32 uniform in [1, 100].  The CSR is symmetric (both arc
+directions) with each adjacency list sorted by neighbour id, which is what the
+reference's ``read_input_graph`` + ``toCSR`` produce
+(graph_hash_of_mixed_weighted_read_for_GSTP.h:75-148, csr_graph.hpp:39-128).
+"""
+from __future__ import annotations
+
+import dataclasses
+import numpy as np
+
+
+@dataclasses.dataclass
+class Graph:
+    V: int
+    beg_pos: np.ndarray  # uint32 [V+1]
+    csr: np.ndarray      # uint32 [arcs]
+    weight: np.ndarray   # int32  [arcs]
+
+    @property
+    def arcs(self) -> int:
+        return int(self.beg_pos[-1])
+
+    def edges(self):
+        """Undirected edge list (u < v) with weights."""
+        src = np.repeat(np.arange(self.V, dtype=np.int64), np.diff(self.beg_pos.astype(np.int64)))
+        m = src < self.csr
+        return src[m], self.csr[m].astype(np.int64), self.weight[m]
+
+
+@dataclasses.dataclass
+class Groups:
+    ptr: np.ndarray      # uint64 [n_groups+1]
+    members: np.ndarray  # uint32 [ptr[-1]], sorted within each group
+
+    @property
+    def n_groups(self) -> int:
+        return len(self.ptr) - 1
+
+    def group(self, g: int) -> np.ndarray:
+        return self.members[self.ptr[g]:self.ptr[g + 1]]
+
+
+def csr_from_edges(V: int, u: np.ndarray, v: np.ndarray, w: np.ndarray) -> Graph:
+    """Symmetric CSR, adjacency sorted by neighbour id."""
+    u = np.asarray(u, dtype=np.int64)
+    v = np.asarray(v, dtype=np.int64)
+    w = np.asarray(w, dtype=np.int32)
+    src = np.concatenate([u, v])
+    dst = np.concatenate([v, u])
+    ww = np.concatenate([w, w])
+    order = np.lexsort((dst, src))
+    src, dst, ww = src[order], dst[order], ww[order]
+    counts = np.bincount(src, minlength=V)
+    beg = np.zeros(V + 1, dtype=np.uint64)
+    np.cumsum(counts, out=beg[1:])
+    if beg[-1] >= 2**32:
+        raise ValueError("arc count exceeds uint32 offsets")
+    return Graph(V, beg.astype(np.uint32), dst.astype(np.uint32), ww)
+
+
+def _unique_edges(V: int, a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    keep = a != b
+    a, b = a[keep], b[keep]
+    lo = np.minimum(a, b).astype(np.int64)
+    hi = np.maximum(a, b).astype(np.int64)
+    return np.unique(lo * V + hi)
+
+
+def chung_lu(V: int, E: int, gamma: float, seed: int, wmax: int = 100) -> Graph:
+    rng = np.random.default_rng(seed)
+    beta = 1.0 / (gamma - 1.0)
+    dmax = min(2.0 * np.sqrt(2.0 * E), V / 2.0)
+    davg = 2.0 * E / V
+    # choose i0 so that w_0 / mean(w) ~= dmax / davg (bisection on log i0)
+    idx = np.arange(V, dtype=np.float64)
+
+    def ratio(i0):
+        w = (idx + i0) ** (-beta)
+        return w[0] / w.mean()
+
+    lo, hi = 0.0, float(V)
+    target = dmax / davg
+    for _ in range(60):
+        mid = 0.5 * (lo + hi)
+        if ratio(mid) > target:
+            lo = mid
+        else:
+            hi = mid
+    i0 = 0.5 * (lo + hi)
+    wts = (idx + i0) ** (-beta)
+    cdf = np.cumsum(wts)
+    cdf /= cdf[-1]
+    keys = np.empty(0, dtype=np.int64)
+    need = E
+    while True:
+        n = int(need * 1.15) + 1024
+        a = np.searchsorted(cdf, rng.random(n), side="right")
+        b = np.searchsorted(cdf, rng.random(n), side="right")
+        a = np.minimum(a, V - 1)
+        b = np.minimum(b, V - 1)
+        keys = np.union1d(keys, _unique_edges(V, a, b))
+        if len(keys) >= E:
+            break
+        need = E - len(keys)
+    if len(keys) > E:
+        keys = np.sort(rng.permutation(keys)[:E])
+    u = keys // V
+    v = keys % V
+    w = rng.integers(1, wmax + 1, size=len(keys), dtype=np.int32)
+    return csr_from_edges(V, u, v, w)
+
+
+def rmat(scale: int, E: int, seed: int, a=0.57, b=0.19, c=0.19, wmax: int = 100) -> Graph:
+    rng = np.random.default_rng(seed)
+    V = 1 << scale
+    perm = rng.permutation(V).astype(np.int64)
+    keys = np.empty(0, dtype=np.int64)
+    need = E
+    while True:
+        n = int(need * 1.6) + 1024
+        src = np.zeros(n, dtype=np.int64)
+        dst = np.zeros(n, dtype=np.int64)
+        for _ in range(scale):
+            r = rng.random(n)
+            sbit = (r >= a + b).astype(np.int64)            # quadrants c, d
+            dbit = (((r >= a) & (r < a + b)) | (r >= a + b + c)).astype(np.int64)  # b, d
+            src = (src << 1) | sbit
+            dst = (dst << 1) | dbit
+        keys = np.union1d(keys, _unique_edges(V, perm[src], perm[dst]))
+        if len(keys) >= E:
+            break
+        need = E - len(keys)
+    if len(keys) > E:
+        keys = np.sort(rng.permutation(keys)[:E])
+    u = keys // V
+    v = keys % V
+    w = rng.integers(1, wmax + 1, size=len(keys), dtype=np.int32)
+    return csr_from_edges(V, u, v, w)
+
+
+def zipf_groups(V: int, n_groups: int, s: float, smax: int, seed: int) -> Groups:
+    rng = np.random.default_rng(seed)
+    ks = np.arange(1, smax + 1, dtype=np.float64)
+    p = ks ** (-s)
+    p /= p.sum()
+    sizes = rng.choice(np.arange(1, smax + 1), size=n_groups, p=p).astype(np.int64)
+    total = int(sizes.sum())
+    gid = np.repeat(np.arange(n_groups, dtype=np.int64), sizes)
+    mem = rng.integers(0, V, size=total, dtype=np.int64)
+    # redraw duplicates inside a group until none remain
+    while True:
+        key = gid * V + mem
+        order = np.argsort(key, kind="stable")
+        ks_sorted = key[order]
+        dup = np.zeros(total, dtype=bool)
+        dup[order[1:]] = ks_sorted[1:] == ks_sorted[:-1]
+        nd = int(dup.sum())
+        if nd == 0:
+            break
+        mem[dup] = rng.integers(0, V, size=nd, dtype=np.int64)
+    covered = np.zeros(V, dtype=bool)
+    covered[mem] = True
+    unc = np.flatnonzero(~covered).astype(np.int64)
+    if len(unc):
+        extra_g = rng.integers(0, n_groups, size=len(unc), dtype=np.int64)
+        gid = np.concatenate([gid, extra_g])
+        mem = np.concatenate([mem, unc])
+    order = np.lexsort((mem, gid))
+    gid, mem = gid[order], mem[order]
+    counts = np.bincount(gid, minlength=n_groups)
+    ptr = np.zeros(n_groups + 1, dtype=np.uint64)
+    np.cumsum(counts, out=ptr[1:])
+    return Groups(ptr, mem.astype(np.uint32))
+
+
+def queries(n_groups: int, n: int, k: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    out = np.empty((n, k), dtype=np.uint32)
+    for i in range(n):
+        out[i] = rng.choice(n_groups, size=k, replace=False)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# The workloads (sizes from the reference benchmark descriptions).
+# ---------------------------------------------------------------------------
+
+def config1(seed: int = 1):
+    """V=10k, E=50k Chung-Lu (gamma 2.5); 2,000 Zipf(1.5) groups in [1,50]; 50 queries k=3."""
+    g = chung_lu(10_000, 50_000, 2.5, seed=1000 + seed)
+    gr = zipf_groups(g.V, 2_000, 1.5, 50, seed=2000 + seed)
+    q = queries(gr.n_groups, 50, 3, seed=3000 + seed)
+    return g, gr, {3: q}
+
+
+def config2(seed: int = 2, n_per_k: int = 300):
+    """V=170k, E=6.8M Chung-Lu (gamma 2.3); 200k Zipf(1.5) groups in [1,200]; 300 queries at each k=3,4,5."""
+    g = chung_lu(170_000, 6_800_000, 2.3, seed=1000 + seed)
+    gr = zipf_groups(g.V, 200_000, 1.5, 200, seed=2000 + seed)
+    qs = {k: queries(gr.n_groups, n_per_k, k, seed=3000 + 10 * seed + k) for k in (3, 4, 5)}
+    return g, gr, qs
+
+
+def config3(seed: int = 3, n_per_cell: int = 100):
+    """R-MAT scale 20, E~10M; 500k Zipf(1.5) groups in [1,200]; k in {3,4,5} x D in {2,3,4}."""
+    g = rmat(20, 10_000_000, seed=1000 + seed)
+    gr = zipf_groups(g.V, 500_000, 1.5, 200, seed=2000 + seed)
+    qs = {(k, D): queries(gr.n_groups, n_per_cell, k, seed=3000 + 100 * seed + 10 * k + D)
+          for k in (3, 4, 5) for D in (2, 3, 4)}
+    return g, gr, qs
+
+
+def small_instance(V: int, E: int, n_groups: int, smax: int, seed: int, gamma: float = 2.5):
+    """Small seeded Chung-Lu instance for parity tests."""
+    E = min(E, V * (V - 1) // 2)
+    g = chung_lu(V, E, gamma, seed=seed)
+    gr = zipf_groups(V, n_groups, 1.5, smax, seed=seed + 7)
+    return g, gr

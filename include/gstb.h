@@ -1,0 +1,140 @@
+/*
+ * gstb -- B200-native exact group Steiner tree (GST) engine, C ABI.
+ *
+ * Drop-in for the query path of the reference (toziki/GPUGST).  The reference
+ * exposes no library API: its query surface is the C++ function
+ *
+ *   void DPBF_GPU(node** host_tree, node* host_tree_one_d, CSR_graph& graph,
+ *                 std::vector<int>& query_groups, graph_v_of_v_idealID& group_graph,
+ *                 graph_v_of_v_idealID& input_graph, int& real_cost,
+ *                 non_overlapped_group_sets s, double& rt, int& RAM, records& ret);
+ *                                                  (code/GPUGST/include/DPQ.cuh:63)
+ *   graph_hash_of_mixed_weighted DPBF_gpu(CSR_graph&, std::vector<int>& query_groups,
+ *                 graph_v_of_v_idealID& group_graph, graph_v_of_v_idealID& input_graph,
+ *                 int D, double* rt, int& real_cost, int& RAM, records&);
+ *                                                  (code/D-GPUGST/include/DPQ.cuh:63)
+ *
+ * called once per query from the experiment drivers
+ * (code/GPUGST/include/exp_GPU_nonHop.h:124, code/D-GPUGST/include/exp_GPU_Hop.h).
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions: plain pointers and sizes only; the caller owns every host
+ * buffer; the library owns every device buffer.  Costs are int32 edge-weight
+ * sums; vertex ids are uint32; a query names k (1..8) group indices (0-based,
+ * i.e. the `.g` file id minus one, as read_Group does at
+ * graph_hash_of_mixed_weighted_read_for_GSTP.h:206).  D < 0 means no hop bound;
+ * 0 <= D <= 7 bounds the tree's hop diameter (the recurrence of
+ * code/D-PrunedDP++/include/CPUHOP.h:192-227: grow d -> d+1 while d < D, merge
+ * with d1 + d2 <= D into max(d1, d2)).
+ */
+#ifndef GSTB_H
+#define GSTB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  Replace the reference's exit(1) / "can not find" prints
+ * (DPQ.cuh:24-41, DPQ.cu:495-500,571-575) and its two conflicting "no
+ * solution" encodings (cost 0 on GPU, 100000 on CPU). */
+typedef enum gst_status {
+  GST_OK = 0,
+  GST_NO_SOLUTION = 1,      /* the query groups are not connected */
+  GST_BAD_INPUT = 2,        /* malformed graph / group index / query */
+  GST_OOM = 3,              /* device memory for the state table not available */
+  GST_DEVICE_TIMEOUT = 4,   /* a bounded device wait expired */
+  GST_CUDA_ERROR = 5,       /* a CUDA runtime call failed */
+  GST_QUEUE_OVERFLOW = 6,   /* a frontier exceeded its capacity */
+  GST_TRUNCATED = 7,        /* tree has more edges than the caller's buffer */
+  GST_INTERNAL = 8,         /* internal consistency check failed */
+  GST_BUSY = 9,             /* serving: no free slot right now (submit again) */
+  GST_NOT_FOUND = 10        /* serving: unknown request id */
+} gst_status;
+
+typedef struct gst_graph gst_graph;
+
+/* Statistics of one query (the reference's CSV columns `counts` and
+ * `process_num`, exp_GPU_nonHop.h:87, plus device counters). */
+enum {
+  GST_STAT_EXPANDED = 0,    /* DP states expanded (reference process_num, DPQ.cu:514) */
+  GST_STAT_SSSP_ITEMS = 1,  /* distance items expanded */
+  GST_STAT_ARCS = 2,        /* arcs scanned (grow + distance) */
+  GST_STAT_UPDATES = 3,     /* successful atomic lowerings */
+  GST_STAT_ENQUEUED = 4,    /* frontier insertions */
+  GST_STAT_ROUNDS = 5,      /* device rounds */
+  GST_STAT_MERGES = 6,      /* merge candidates evaluated */
+  GST_STAT_TABLE_BYTES = 7, /* bytes of the state table */
+  GST_NSTATS = 8
+};
+
+typedef struct gst_result {
+  int32_t cost;            /* optimal cost (valid when status == GST_OK) */
+  uint32_t root;           /* root vertex of the returned tree */
+  int32_t n_edges;         /* number of tree edges (may exceed max_edges: TRUNCATED) */
+  int32_t max_edges;       /* capacity of `edges` in edges (caller sets) */
+  uint32_t* edges;         /* caller buffer, 3*max_edges uint32: (u, v, w) triples */
+  uint64_t stats[GST_NSTATS];
+  double device_ms;        /* device time of the query (CUDA events) */
+} gst_result;
+
+/* Replaces toCSR (code/GPUGST/include/graph_v_of_v_idealID/csr_graph.hpp:39-128):
+ * copies a symmetric CSR (beg_pos[V+1], csr[arcs], w[arcs]; both directions
+ * of every undirected edge present; weights >= 1) to the device.  The library
+ * keeps its own device copy with each adjacency list re-sorted by weight. */
+gst_status gst_graph_create(const uint32_t* beg_pos, const uint32_t* csr, const int32_t* w,
+                            uint32_t V, uint64_t arcs, gst_graph** out);
+
+/* Replaces read_Group's group_graph (graph_hash_of_mixed_weighted_read_for_GSTP.h:190-239):
+ * group g has members grp_v[grp_ptr[g] .. grp_ptr[g+1]).  Copied to the device. */
+gst_status gst_groups_set(gst_graph* g, const uint64_t* grp_ptr, const uint32_t* grp_v,
+                          uint32_t n_groups);
+
+void gst_graph_destroy(gst_graph* g);
+
+uint32_t gst_graph_num_vertices(const gst_graph* g);
+uint64_t gst_graph_num_arcs(const gst_graph* g);
+
+/* Replaces DPBF_GPU (code/GPUGST/include/DPQ.cuh:63, DPQ.cu:275-624) when D < 0
+ * and DPBF_gpu (code/D-GPUGST/include/DPQ.cuh:63, D-GPUGST/src/DPQ.cu:149-269)
+ * when D >= 0.  One synchronous query; returns the exact optimum cost and a
+ * tree (the reference's GPU path returns the cost only; its extraction is
+ * commented out at DPQ.cu:577-606). */
+gst_status gst_query(gst_graph* g, const uint32_t* groups, int k, int D, gst_result* out);
+
+/* Batched launch: n queries share the device rounds.  groups[i*8 .. i*8+ks[i])
+ * lists query i's groups.  results[i].edges/max_edges set by the caller.
+ * statuses[i] receives each query's status.  Queries are admitted by the HBM
+ * bytes of their state tables; at most max_concurrent run at once (0 = as
+ * many as fit). */
+gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const int32_t* ks,
+                           const int32_t* Ds, gst_result* results, int32_t* statuses,
+                           int max_concurrent);
+
+/* Serving loop (continuous batching).  A background host thread keeps the
+ * graph resident, admits submitted queries as device memory frees up, and
+ * runs every admitted query's rounds together.  No reference counterpart
+ * (the reference runs queries serially, exp_GPU_nonHop.h:97-138). */
+typedef struct gst_server gst_server;
+
+gst_status gst_serve_open(gst_graph* g, uint64_t hbm_budget_bytes, int max_inflight,
+                          gst_server** out);
+/* Never blocks.  Copies the groups.  GST_BUSY if the pending queue is full. */
+gst_status gst_serve_submit(gst_server* s, uint64_t req_id, const uint32_t* groups, int k, int D);
+/* Returns up to max_results finished requests; *n_out set.  Tree edges are
+ * copied into each result's caller buffer (edges/max_edges preset by the
+ * caller; pass max_edges 0 to skip trees).  ids[i] and statuses[i] filled. */
+gst_status gst_serve_poll(gst_server* s, uint64_t* ids, int32_t* statuses, gst_result* results,
+                          int max_results, int* n_out);
+/* Host timestamps of a finished request, valid after poll: submit -> done (ms). */
+gst_status gst_serve_close(gst_server* s);
+
+const char* gst_status_string(gst_status st);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSTB_H */

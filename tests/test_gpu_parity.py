@@ -1,0 +1,165 @@
+"""GPU path (through the C ABI) against the CPU oracle on the same seeded inputs.
+
+Costs must match bit for bit; every returned tree must pass the validator
+(edges exist with their weights, connected, acyclic, covers every query group,
+weights sum to the cost, hop diameter <= D)."""
+import numpy as np
+import pytest
+
+from gpugst_b200 import gen
+from tests.cases import small_cases, tiny_cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _engine(eng, g, gr):
+    return eng.Engine.from_instance(g, gr)
+
+
+def test_tiny_vs_brute(gst_lib, oracle_mod):
+    eng, O = gst_lib, oracle_mod
+    bad = []
+    for i, (g, gr, q, D) in enumerate(tiny_cases(160)):
+        E = _engine(eng, g, gr)
+        for DD in (-1, D):
+            want = O.brute(g, gr, q, DD)
+            r = E.query(q, D=DD)
+            if want < 0:
+                if r.status != eng.GST_NO_SOLUTION:
+                    bad.append((i, DD, "want no solution", r.status, r.cost))
+                continue
+            if r.status != eng.GST_OK or r.cost != want:
+                bad.append((i, DD, want, r.status, r.cost))
+                continue
+            v = O.validate(g, gr, q, DD, r.cost, r.root, r.edges)
+            if v:
+                bad.append((i, DD, "invalid tree", v))
+        E.close()
+    assert not bad, bad[:10]
+
+
+def test_small_plain_vs_oracle(gst_lib, oracle_mod):
+    eng, O = gst_lib, oracle_mod
+    bad = []
+    for i, (g, gr, q) in enumerate(small_cases(24)):
+        E = _engine(eng, g, gr)
+        want = O.prunedpp(g, gr, q, 0)
+        r = E.query(q)
+        if want.status != 0:
+            if r.status != eng.GST_NO_SOLUTION:
+                bad.append((i, "no-solution", r.status))
+        elif r.status != eng.GST_OK or r.cost != want.cost:
+            bad.append((i, want.cost, r.status, r.cost))
+        elif O.validate(g, gr, q, -1, r.cost, r.root, r.edges):
+            bad.append((i, "invalid tree"))
+        E.close()
+    assert not bad, bad
+
+
+def test_small_hop_vs_oracle(gst_lib, oracle_mod):
+    eng, O = gst_lib, oracle_mod
+    bad = []
+    for i, (g, gr, q) in enumerate(small_cases(16, seed0=300, V=200, E=800, kmax=4)):
+        E = _engine(eng, g, gr)
+        for D in (1, 2, 3, 4):
+            want = O.hop(g, gr, q, D)
+            r = E.query(q, D=D)
+            if want.status != 0:
+                if r.status != eng.GST_NO_SOLUTION:
+                    bad.append((i, D, "no-solution", r.status, r.cost))
+            elif r.status != eng.GST_OK or r.cost != want.cost:
+                bad.append((i, D, want.cost, r.status, r.cost))
+            elif O.validate(g, gr, q, D, r.cost, r.root, r.edges):
+                bad.append((i, D, "invalid tree"))
+        E.close()
+    assert not bad, bad
+
+
+@pytest.fixture(scope="module")
+def c1():
+    return gen.config1()
+
+
+def test_config1_plain(gst_lib, oracle_mod, c1):
+    eng, O = gst_lib, oracle_mod
+    g, gr, qs = c1
+    E = _engine(eng, g, gr)
+    bad = []
+    for i, q in enumerate(qs[3]):
+        want = O.prunedpp(g, gr, q, 0)
+        r = E.query(q)
+        if r.status != eng.GST_OK or r.cost != want.cost:
+            bad.append((i, want.cost, r.status, r.cost))
+        elif O.validate(g, gr, q, -1, r.cost, r.root, r.edges):
+            bad.append((i, "invalid tree"))
+    E.close()
+    assert not bad, bad
+
+
+def test_config1_hop(gst_lib, oracle_mod, c1):
+    eng, O = gst_lib, oracle_mod
+    g, gr, qs = c1
+    E = _engine(eng, g, gr)
+    bad = []
+    for i, q in enumerate(qs[3][:12]):
+        for D in (2, 3, 4):
+            want = O.hop(g, gr, q, D)
+            r = E.query(q, D=D)
+            if want.status != 0:
+                if r.status != eng.GST_NO_SOLUTION:
+                    bad.append((i, D, "no-solution", r.status, r.cost))
+            elif r.status != eng.GST_OK or r.cost != want.cost:
+                bad.append((i, D, want.cost, r.status, r.cost))
+            elif O.validate(g, gr, q, D, r.cost, r.root, r.edges):
+                bad.append((i, D, "invalid tree"))
+    E.close()
+    assert not bad, bad
+
+
+def test_batch_alone_vs_mixed(gst_lib, c1):
+    """Each query gives the same cost alone and inside a mixed batch."""
+    eng = gst_lib
+    g, gr, qs = c1
+    rng = np.random.default_rng(5)
+    queries, Ds = [], []
+    for i in range(40):
+        k = int(rng.integers(2, 6))
+        queries.append(rng.choice(gr.n_groups, size=k, replace=False).astype(np.uint32))
+        Ds.append(int(rng.choice([-1, 2, 3, 4])))
+    E = _engine(eng, g, gr)
+    alone = [E.query(q, D=D) for q, D in zip(queries, Ds)]
+    mixed = E.query_batch(queries, Ds)
+    E.close()
+    for a, m in zip(alone, mixed):
+        assert a.status == m.status
+        assert a.cost == m.cost
+
+
+def test_edge_cases(gst_lib, oracle_mod):
+    eng, O = gst_lib, oracle_mod
+    # path 0-1-2-3 plus isolated vertex 4
+    u = np.array([0, 1, 2]); v = np.array([1, 2, 3]); w = np.array([5, 7, 11], dtype=np.int32)
+    g = gen.csr_from_edges(5, u, v, w)
+    ptr = np.array([0, 1, 2, 3, 4, 6, 7], dtype=np.uint64)
+    mem = np.array([0, 3, 1, 4, 0, 3, 2], dtype=np.uint32)
+    gr = gen.Groups(ptr, mem)
+    E = eng.Engine.from_instance(g, gr)
+    r = E.query([0])                      # k = 1: a single member vertex
+    assert r.ok and r.cost == 0 and len(r.edges) == 0
+    r = E.query([0, 4])                   # vertex 0 is in both groups
+    assert r.ok and r.cost == 0
+    r = E.query([0, 1])                   # 0 .. 3 along the path
+    assert r.ok and r.cost == 23 and O.validate(g, gr, np.array([0, 1]), -1, r.cost, r.root, r.edges) == 0
+    r = E.query([0, 1], D=2)              # needs 3 hops
+    assert r.status == eng.GST_NO_SOLUTION
+    r = E.query([0, 1], D=3)
+    assert r.ok and r.cost == 23
+    r = E.query([0, 3])                   # group 3 = {4}, isolated
+    assert r.status == eng.GST_NO_SOLUTION
+    r = E.query([1, 2, 5])
+    assert r.ok and r.cost == O.prunedpp(g, gr, np.array([1, 2, 5]), 0).cost
+    for bad_q, bad_d in (([], -1), ([0] * 9, -1), ([0, 0], -1), ([0, 99], -1), ([0, 1], 8)):
+        r = E.query(bad_q, D=bad_d) if bad_q else None
+        if r is not None:
+            assert r.status == eng.GST_BAD_INPUT, (bad_q, bad_d, r.status)
+    E.close()

@@ -1,0 +1,78 @@
+"""The CPU oracle against itself, brute force and the generators (no GPU)."""
+import numpy as np
+import pytest
+
+from gpugst_b200 import gen
+from tests.cases import tiny_cases
+
+
+def test_generators_shape():
+    g, gr, qs = gen.config1()
+    assert g.V == 10_000 and g.arcs == 100_000
+    deg = np.diff(g.beg_pos.astype(np.int64))
+    src = np.repeat(np.arange(g.V), deg)
+    assert (src != g.csr).all(), "self-loop"
+    # adjacency sorted by neighbour, no duplicates
+    for v in range(0, g.V, 97):
+        row = g.csr[g.beg_pos[v]:g.beg_pos[v + 1]]
+        assert (np.diff(row.astype(np.int64)) > 0).all()
+    # symmetric with equal weights
+    key = src * g.V + g.csr.astype(np.int64)
+    rkey = g.csr.astype(np.int64) * g.V + src
+    order = np.argsort(key)
+    rorder = np.argsort(rkey)
+    assert (key[order] == rkey[rorder]).all()
+    assert (g.weight[order] == g.weight[rorder]).all()
+    assert g.weight.min() >= 1 and g.weight.max() <= 100
+    assert gr.n_groups == 2000
+    cov = np.zeros(g.V, bool)
+    cov[gr.members] = True
+    assert cov.all(), "every vertex is in a group"
+    sizes = np.diff(gr.ptr.astype(np.int64))
+    assert sizes.min() >= 1
+    assert qs[3].shape == (50, 3)
+    for q in qs[3]:
+        assert len(set(q.tolist())) == 3
+
+
+@pytest.mark.parametrize("chunk", range(4))
+def test_oracle_tiny_vs_brute(oracle_mod, chunk):
+    O = oracle_mod
+    for g, gr, q, D in tiny_cases(60, seed0=chunk * 60):
+        b = O.brute(g, gr, q)
+        p = O.prunedpp(g, gr, q, 0)
+        d = O.dpbf(g, gr, q)
+        assert b == p.cost == d.cost
+        if b >= 0:
+            assert O.validate(g, gr, q, -1, p.cost, p.root, p.edges) == 0
+            assert O.validate(g, gr, q, -1, d.cost, d.root, d.edges) == 0
+        bh = O.brute(g, gr, q, D)
+        h = O.hop(g, gr, q, D)
+        assert bh == h.cost
+        if bh >= 0:
+            assert O.validate(g, gr, q, D, h.cost, h.root, h.edges) == 0
+
+
+def test_oracle_config1_exact_modes(oracle_mod):
+    """PrunedDP++ with ratio 0 (exact exits only) equals plain DPBF."""
+    O = oracle_mod
+    g, gr, qs = gen.config1()
+    for q in qs[3][:25]:
+        a = O.prunedpp(g, gr, q, 0)
+        b = O.dpbf(g, gr, q)
+        assert a.cost == b.cost
+        assert O.validate(g, gr, q, -1, a.cost, a.root, a.edges) == 0
+
+
+def test_validator_rejects(oracle_mod):
+    O = oracle_mod
+    g, gr, qs = gen.config1()
+    q = qs[3][0]
+    r = O.prunedpp(g, gr, q, 0)
+    assert O.validate(g, gr, q, -1, r.cost, r.root, r.edges) == 0
+    assert O.validate(g, gr, q, -1, r.cost + 1, r.root, r.edges) == 4
+    if len(r.edges) > 1:
+        assert O.validate(g, gr, q, -1, r.cost, r.root, r.edges[1:]) != 0
+        bad = r.edges.copy()
+        bad[0, 2] += 1
+        assert O.validate(g, gr, q, -1, r.cost, r.root, bad) == 1
