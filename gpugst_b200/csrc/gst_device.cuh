@@ -11,7 +11,7 @@
 //   dflag  u32 [ceil(V*2^k*nd/16)]  2 bits per state: in-near, in-far
 //   sflag  u32 [ceil(V*8/16)]      2 bits per distance item
 //   qbuf   u32 [4][cap]        near-in, near-out, far, far-out work lists of state ids
-//   tour   u32 [k][2^k][k] + [k][2^k]   group-tour tables P and T2 (lower bounds)
+//   tour   u32 [k][2^k][k] + [k][2^k] + [8][8]  tour tables P, T2 and group distances
 #pragma once
 #include <cstdint>
 
@@ -24,6 +24,24 @@ constexpr uint32_t PAR_GROW = 0x40000000u;
 constexpr uint32_t PAR_MERGE = 0x80000000u;
 constexpr int KMAX = 8;
 constexpr int DMAX = 7;
+
+// Job state machine (advanced on the device by k_control once per round).
+enum JobState : int32_t { J_FREE = 0, J_INIT, J_SSSP, J_TOUR, J_DPSEED, J_DP, J_EXTRACT, J_DONE };
+enum Action : int32_t { A_NONE = 0, A_SSEED, A_WORK, A_SPLIT, A_TOUR, A_DSEED, A_EXTRACT };
+
+// Task types of one round.  Light kernel: split, seeds, tour, extract and
+// distance items; heavy kernel: DP items.
+enum TaskType : int32_t { T_SPLIT = 0, T_SSEED, T_DSEED, T_TOUR, T_EXTRACT, T_SSSP, T_DP, T_HOP, NT };
+constexpr int MAX_SLOTS = 1024;
+
+// Round-wide work description written by k_control.
+struct RoundDesc {
+  uint32_t items[NT];     // items per task type
+  uint32_t task_off[NT + 1];  // warp-task offsets (light types, then heavy types restart at 0)
+  uint32_t light_tasks, heavy_tasks;
+  uint32_t n_live;        // slots whose job is not finished
+  uint32_t pad;
+};
 
 enum Phase : int32_t {
   PH_IDLE = 0,
@@ -55,6 +73,9 @@ struct alignas(16) QCtl {
   uint32_t root;
   unsigned long long best_full;  // min over full states of cost << 32 | payload
   unsigned long long stat[8];
+  uint32_t done;     // job finished (set by k_control)
+  uint32_t final_status;  // gst_status of the finished job
+  uint32_t pad[2];
 };
 
 // Per-query descriptor; the host rewrites it before each round.
@@ -80,6 +101,10 @@ struct QDev {
   uint32_t n_far;    // items in qbuf[far_idx] (split input)
   uint32_t theta_lo, theta_hi;  // current near window [lo, hi)
   uint32_t cap1;     // distances >= cap1 are only known to be >= cap1
+  uint32_t cap_num, cap_den;  // distance rounds stop at best * cap_num / cap_den
+  // state machine
+  int32_t st, act;
+  uint32_t delta, delta_sssp, delta_dp;
 };
 
 struct GraphDev {

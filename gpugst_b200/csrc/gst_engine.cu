@@ -28,12 +28,9 @@
 #include "gst_device.cuh"
 
 namespace gstb {
-__global__ void k_work(const QDev*, const uint32_t*, const uint32_t*, int, uint32_t, GraphDev);
-__global__ void k_split(const QDev*, const uint32_t*, const uint32_t*, int, uint32_t);
-__global__ void k_sssp_seed(const QDev*, const uint32_t*, const uint32_t*, int, uint32_t);
-__global__ void k_dp_seed(const QDev*, const uint32_t*, const uint32_t*, int, uint32_t);
-__global__ void k_tour(const QDev*, const uint32_t*);
-__global__ void k_extract(const QDev*, const uint32_t*, int, GraphDev);
+__global__ void k_control(QDev*, QCtl*, int, RoundDesc*, uint32_t*);
+__global__ void k_light(const QDev*, const RoundDesc*, const uint32_t*, int, GraphDev);
+__global__ void k_heavy(const QDev*, const RoundDesc*, const uint32_t*, int, GraphDev);
 }  // namespace gstb
 
 using namespace gstb;
@@ -62,6 +59,14 @@ struct gst_graph {
   std::vector<uint32_t> grp_v;
   int device = 0;
   int num_sms = 148;
+  // persistent round driver for gst_query / gst_query_batch (created lazily)
+  void* runner = nullptr;
+  std::mutex mu;
+  std::atomic<uint64_t> launches{0};
+  bool profile = false;
+  double prof_work_ms = 0;
+  uint64_t prof_work_launches = 0;
+  uint64_t prof_stats[GST_NSTATS] = {0};
 };
 
 namespace {
@@ -71,9 +76,6 @@ uint32_t env_u32(const char* name, uint32_t def) {
   if (!s || !*s) return def;
   return (uint32_t)strtoul(s, nullptr, 10);
 }
-
-enum JobState { J_INIT, J_SSSP, J_TOUR, J_DPSEED, J_DP, J_EXTRACT, J_DONE };
-enum Action { A_NONE, A_SSEED, A_WORK, A_SPLIT, A_TOUR, A_DSEED, A_EXTRACT };
 
 struct Job {
   // request
@@ -91,12 +93,9 @@ struct Job {
   QDev qd{};
   QCtl ctl{};
   int slot = -1;
-  JobState st = J_INIT;
-  Action act = A_NONE;
-  uint32_t delta = 1;
   gst_status status = GST_OK;
-  bool rejected = false;      // failed validation before admission
-  uint64_t rounds = 0;
+  bool rejected = false;  // failed validation before admission
+  bool done = false;
   // results
   int32_t cost = -1;
   uint32_t root = 0;
@@ -126,7 +125,7 @@ Layout layout_for(const gst_graph* g, int k, int nd, size_t n_members, uint32_t 
   L.dflag = o; o = align_up(o + ((states + 15) / 16) * 4, 256);
   L.sflag = o; o = align_up(o + (((size_t)g->V * 8 + 15) / 16) * 4, 256);
   L.qbuf = o; o = align_up(o + 4 * cap * 4, 256);
-  L.tour = o; o = align_up(o + ((size_t)k * (1u << k) * k + (size_t)k * (1u << k)) * 4, 256);
+  L.tour = o; o = align_up(o + ((size_t)k * (1u << k) * k + (size_t)k * (1u << k) + 64) * 4, 256);
   L.members = o; o = align_up(o + std::max<size_t>(n_members, 1) * 4, 256);
   L.edges = o; o = align_up(o + (size_t)std::max<uint32_t>(max_edges, 1) * 12, 256);
   L.total = o;
@@ -134,7 +133,10 @@ Layout layout_for(const gst_graph* g, int k, int nd, size_t n_members, uint32_t 
 }
 
 // ---------------------------------------------------------------------------
-// Round driver
+// Round driver.  Queries occupy slots of device-resident descriptors; every
+// round is k_control -> k_light -> k_heavy, all reading their work from device
+// memory, so the host launches several rounds back to back and synchronises
+// only to admit new queries and retire finished ones.
 // ---------------------------------------------------------------------------
 class Runner {
  public:
@@ -144,32 +146,57 @@ class Runner {
   gst_status init() {
     CK(cudaSetDevice(g_->device));
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    for (auto& e : ev_) CK(cudaEventCreate(&e));
     cudaMemPool_t pool;
     CK(cudaDeviceGetDefaultMemPool(&pool, g_->device));
     uint64_t thr = ~0ull;
     CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
-    delta_sssp_ = env_u32("GSTB_DELTA_SSSP", 4);
-    delta_dp_ = env_u32("GSTB_DELTA_DP", 2);
+    delta_sssp_ = std::max(1u, env_u32("GSTB_DELTA_SSSP", 8));
+    delta_dp_ = std::max(1u, env_u32("GSTB_DELTA_DP", 2));
+    cap_num_ = std::max(1u, env_u32("GSTB_SSSP_CAP_NUM", 1));
+    cap_den_ = std::max(1u, env_u32("GSTB_SSSP_CAP_DEN", 2));
     max_edges_dev_ = env_u32("GSTB_MAX_TREE_EDGES", 1u << 16);
+    rounds_per_sync_ = std::min(64u, std::max(1u, env_u32("GSTB_ROUNDS_PER_SYNC", 6)));
+    max_slots_ = std::min<uint32_t>(MAX_SLOTS - 1, std::max(1u, env_u32("GSTB_MAX_SLOTS", MAX_SLOTS - 1)));
+    CK(cudaMalloc(&d_qd_, MAX_SLOTS * sizeof(QDev)));
+    CK(cudaMalloc(&d_ctl_, MAX_SLOTS * sizeof(QCtl)));
+    CK(cudaMalloc(&d_rd_, sizeof(RoundDesc)));
+    CK(cudaMalloc(&d_pre_, (size_t)NT * (MAX_SLOTS + 1) * 4));
+    CK(cudaMemset(d_qd_, 0, MAX_SLOTS * sizeof(QDev)));
+    CK(cudaMemset(d_ctl_, 0, MAX_SLOTS * sizeof(QCtl)));
+    CK(cudaMallocHost(&h_ctl_, MAX_SLOTS * sizeof(QCtl)));
+    CK(cudaMallocHost(&h_rd_, sizeof(RoundDesc)));
+    CK(cudaMallocHost(&h_qd_, sizeof(QDev)));
+    slots_.assign(max_slots_, nullptr);
+    int bl = 0, bh = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, k_light, 256, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bh, k_heavy, 256, 0));
+    light_grid_ = (unsigned)g_->num_sms * (unsigned)std::max(1, bl);
+    heavy_grid_ = (unsigned)g_->num_sms * (unsigned)std::max(1, bh);
     return GST_OK;
   }
 
   void release() {
-    for (auto* j : active_) free_job(j);
-    active_.clear();
+    for (Job* j : slots_)
+      if (j) free_job(j);
+    slots_.clear();
     if (d_qd_) cudaFree(d_qd_);
     if (d_ctl_) cudaFree(d_ctl_);
-    if (d_lists_) cudaFree(d_lists_);
+    if (d_rd_) cudaFree(d_rd_);
+    if (d_pre_) cudaFree(d_pre_);
     if (h_ctl_) cudaFreeHost(h_ctl_);
+    if (h_rd_) cudaFreeHost(h_rd_);
     if (h_qd_) cudaFreeHost(h_qd_);
-    if (h_lists_) cudaFreeHost(h_lists_);
+    for (auto& e : ev_)
+      if (e) cudaEventDestroy(e);
     if (stream_) cudaStreamDestroy(stream_);
     d_qd_ = nullptr;
     d_ctl_ = nullptr;
-    d_lists_ = nullptr;
+    d_rd_ = nullptr;
+    d_pre_ = nullptr;
     h_ctl_ = nullptr;
+    h_rd_ = nullptr;
     h_qd_ = nullptr;
-    h_lists_ = nullptr;
     stream_ = nullptr;
   }
 
@@ -200,14 +227,26 @@ class Runner {
     return GST_OK;
   }
 
-  // Allocate the workspace and queue the initial memsets; false if no memory.
+  bool has_free_slot() const { return n_used_ < max_slots_; }
+  size_t live() const { return n_used_; }
+
+  // Allocate the workspace, initialise it and install the job in a free
+  // slot; false if no slot or no device memory is available.
   bool admit(Job* j) {
+    if (n_used_ >= max_slots_) return false;
     void* p = nullptr;
     if (cudaMallocAsync(&p, j->bytes, stream_) != cudaSuccess) {
       cudaGetLastError();
       return false;
     }
+    int slot = -1;
+    for (uint32_t s = 0; s < max_slots_; s++)
+      if (!slots_[s]) {
+        slot = (int)s;
+        break;
+      }
     j->mem = (char*)p;
+    j->slot = slot;
     Layout L = layout_for(g_, j->k, j->nd, j->members.size(), max_edges_dev_);
     QDev& q = j->qd;
     memset(&q, 0, sizeof(q));
@@ -219,6 +258,7 @@ class Runner {
     q.tour = (uint32_t*)(j->mem + L.tour);
     q.members = (const uint32_t*)(j->mem + L.members);
     q.out_edges = (uint32_t*)(j->mem + L.edges);
+    q.ctl = d_ctl_ + slot;
     q.cap = L.cap;
     q.n_members = (uint32_t)j->members.size();
     q.max_edges = max_edges_dev_;
@@ -228,10 +268,16 @@ class Runner {
     q.full = (int)j->full;
     q.WT = j->WT;
     q.phase = PH_SSSP;
+    q.cap_num = cap_num_;
+    q.cap_den = cap_den_;
     q.in_idx = 0;
     q.out_idx = 1;
     q.far_idx = 2;
     q.far2_idx = 3;
+    q.st = J_INIT;
+    q.act = A_NONE;
+    q.delta_sssp = delta_sssp_;
+    q.delta_dp = delta_dp_;
     memset(&j->ctl, 0, sizeof(j->ctl));
     j->ctl.best = INF32;
     j->ctl.best_full = INF64;
@@ -239,9 +285,14 @@ class Runner {
     cudaMemsetAsync(q.dist, 0xFF, (size_t)g_->V * 8 * 4, stream_);
     cudaMemsetAsync(q.dflag, 0, L.sflag - L.dflag, stream_);
     cudaMemsetAsync(q.sflag, 0, L.qbuf - L.sflag, stream_);
-    cudaMemcpyAsync((void*)q.members, j->members.data(), j->members.size() * 4, cudaMemcpyHostToDevice,
-                    stream_);
-    j->st = J_INIT;
+    cudaMemcpyAsync((void*)q.members, j->members.data(), j->members.size() * 4, cudaMemcpyHostToDevice, stream_);
+    // the descriptors are copied from pageable host memory: the call returns
+    // once the source has been staged, so the job's own copies may be reused
+    cudaMemcpyAsync(d_qd_ + slot, &q, sizeof(QDev), cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(d_ctl_ + slot, &j->ctl, sizeof(QCtl), cudaMemcpyHostToDevice, stream_);
+    slots_[slot] = j;
+    n_used_++;
+    nslots_hi_ = std::max<uint32_t>(nslots_hi_, (uint32_t)slot + 1);
     j->t_admit = std::chrono::steady_clock::now();
     return true;
   }
@@ -251,284 +302,110 @@ class Runner {
     j->mem = nullptr;
   }
 
-  // Run rounds until every job in `jobs` is done.  `more` (optional) is
-  // polled between rounds to admit new jobs (serving / batch admission).
-  template <class AdmitFn>
-  gst_status run(AdmitFn&& admit_more) {
+  double last_call_ms() const { return last_call_ms_; }
+
+  // Run rounds until no admitted job is left and admit_more() adds none.
+  // `on_done` is called for every finished job (after its results are copied).
+  template <class AdmitFn, class DoneFn>
+  gst_status run(AdmitFn&& admit_more, DoneFn&& on_done) {
+    CK(cudaEventRecord(ev_[0], stream_));
     for (;;) {
-      admit_more(active_);
-      if (active_.empty()) return GST_OK;
-      gst_status st = round();
-      if (st != GST_OK) return st;
-      // retire finished jobs
-      std::vector<Job*> keep;
-      for (Job* j : active_) {
-        if (j->st == J_DONE) {
-          free_job(j);
-          finished_.push_back(j);
-        } else {
-          keep.push_back(j);
-        }
+      admit_more();
+      if (n_used_ == 0) {
+        CK(cudaEventRecord(ev_[1], stream_));
+        CK(cudaEventSynchronize(ev_[1]));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
+        last_call_ms_ = ms;
+        return GST_OK;
       }
-      active_.swap(keep);
+      gst_status st = rounds(rounds_per_sync_);
+      if (st != GST_OK) return st;
+      st = retire(on_done);
+      if (st != GST_OK) return st;
     }
   }
 
-  std::vector<Job*>& active() { return active_; }
-  std::vector<Job*>& finished() { return finished_; }
-  cudaStream_t stream() const { return stream_; }
-
  private:
-  gst_status ensure_buffers(size_t nj, size_t list_words) {
-    if (nj > cap_jobs_) {
-      size_t n = std::max(nj, cap_jobs_ * 2 + 16);
-      if (d_qd_) cudaFree(d_qd_);
-      if (d_ctl_) cudaFree(d_ctl_);
-      if (h_ctl_) cudaFreeHost(h_ctl_);
-      if (h_qd_) cudaFreeHost(h_qd_);
-      CK(cudaMalloc(&d_qd_, n * sizeof(QDev)));
-      CK(cudaMalloc(&d_ctl_, n * sizeof(QCtl)));
-      CK(cudaMallocHost(&h_ctl_, n * sizeof(QCtl)));
-      CK(cudaMallocHost(&h_qd_, n * sizeof(QDev)));
-      cap_jobs_ = n;
+  gst_status rounds(uint32_t R) {
+    GraphDev gd{g_->d_beg, g_->d_adj, g_->V};
+    const int ns = (int)nslots_hi_;
+    const unsigned light_grid = light_grid_, heavy_grid = heavy_grid_;
+    const bool prof = g_->profile;
+    for (uint32_t r = 0; r < R; r++) {
+      k_control<<<1, 1024, 0, stream_>>>(d_qd_, d_ctl_, ns, d_rd_, d_pre_);
+      if (prof) CK(cudaEventRecord(ev_[2 + 2 * r], stream_));
+      k_light<<<light_grid, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
+      k_heavy<<<heavy_grid, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
+      if (prof) CK(cudaEventRecord(ev_[3 + 2 * r], stream_));
     }
-    if (list_words > cap_lists_) {
-      size_t n = std::max(list_words, cap_lists_ * 2 + 256);
-      if (d_lists_) cudaFree(d_lists_);
-      if (h_lists_) cudaFreeHost(h_lists_);
-      CK(cudaMalloc(&d_lists_, n * 4));
-      CK(cudaMallocHost(&h_lists_, n * 4));
-      cap_lists_ = n;
+    CK(cudaGetLastError());
+    g_->launches += 3ull * R;
+    CK(cudaMemcpyAsync(h_ctl_, d_ctl_, (size_t)ns * sizeof(QCtl), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    if (prof) {
+      for (uint32_t r = 0; r < R; r++) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev_[2 + 2 * r], ev_[3 + 2 * r]));
+        g_->prof_work_ms += ms;
+        g_->prof_work_launches += 2;
+      }
     }
     return GST_OK;
   }
 
-  // Decide this round's action for a job (host state machine).
-  void decide(Job* j) {
-    QDev& q = j->qd;
-    QCtl& c = j->ctl;
-    j->act = A_NONE;
-    for (;;) {
-      switch (j->st) {
-        case J_INIT:
-          q.phase = PH_SSSP;
-          q.theta_lo = 0;
-          q.theta_hi = delta_sssp_;
-          j->delta = delta_sssp_;
-          c.n_near = 0;
-          j->act = A_SSEED;
-          return;
-        case J_SSSP:
-        case J_DP: {
-          if (q.n_in > 0) {
-            c.n_near = 0;
-            c.n_far = q.n_far;
-            j->act = A_WORK;
-            return;
-          }
-          uint32_t next_lo = q.theta_hi;
-          bool exhausted = q.n_far == 0 || next_lo > c.best;
-          if (!exhausted) {
-            q.theta_lo = next_lo;
-            q.theta_hi = next_lo + j->delta;
-            c.n_near = 0;
-            c.n_far2 = 0;
-            j->act = A_SPLIT;
-            return;
-          }
-          if (j->st == J_SSSP) {
-            // every distance below theta_hi is exact, every distance <= best
-            // was discovered; unknown ones are at least min(theta_hi, best+1)
-            uint64_t b1 = c.best == INF32 ? (uint64_t)INF32 : (uint64_t)c.best + 1;
-            uint64_t cap1 = std::min<uint64_t>(q.theta_hi, b1);
-            if (q.n_far == 0) cap1 = b1;  // nothing pending: all reachable distances are final
-            q.cap1 = (uint32_t)std::min<uint64_t>(cap1, BIG);
-            j->st = J_TOUR;
-            continue;
-          }
-          j->st = J_EXTRACT;
-          continue;
-        }
-        case J_TOUR:
-          j->act = A_TOUR;
-          return;
-        case J_DPSEED:
-          q.phase = j->D < 0 ? PH_DP : PH_HOP;
-          q.theta_lo = 0;
-          q.theta_hi = delta_dp_;
-          j->delta = delta_dp_;
-          q.n_in = 0;
-          q.n_far = 0;
-          c.n_near = 0;
-          c.n_far = 0;
-          j->act = A_DSEED;
-          return;
-        case J_EXTRACT:
-          j->act = A_EXTRACT;
-          return;
-        case J_DONE:
-          return;
-      }
-    }
-  }
-
-  // Apply the effects of this round's action after the control blocks are back.
-  void absorb(Job* j) {
-    QDev& q = j->qd;
-    QCtl& c = j->ctl;
-    if (c.overflow) {
-      j->status = GST_QUEUE_OVERFLOW;
-      j->st = J_DONE;
-      finish_timestamps(j);
-      return;
-    }
-    switch (j->act) {
-      case A_SSEED:
-        std::swap(q.in_idx, q.out_idx);
-        q.n_in = c.n_near;
-        q.n_far = 0;
-        j->st = J_SSSP;
-        break;
-      case A_WORK:
-        std::swap(q.in_idx, q.out_idx);
-        q.n_in = c.n_near;
-        q.n_far = c.n_far;
-        break;
-      case A_SPLIT:
-        std::swap(q.in_idx, q.out_idx);
-        std::swap(q.far_idx, q.far2_idx);
-        q.n_in = c.n_near;
-        q.n_far = c.n_far2;
-        break;
-      case A_TOUR:
-        j->st = J_DPSEED;
-        break;
-      case A_DSEED:
-        std::swap(q.in_idx, q.out_idx);
-        q.n_in = c.n_near;
-        q.n_far = 0;
-        j->st = J_DP;
-        break;
-      case A_EXTRACT:
-        j->st = J_DONE;
-        if (c.status == 1) {
-          j->status = GST_NO_SOLUTION;
-        } else if (c.status != 0) {
-          j->status = GST_INTERNAL;
-        } else {
-          j->status = GST_OK;
-          j->cost = (int32_t)(c.best_full >> 32);
-          j->root = c.root;
-        }
-        break;
-      default:
-        break;
-    }
-    if (j->act != A_NONE) j->rounds++;
-  }
-
-  void finish_timestamps(Job* j) { j->t_done = std::chrono::steady_clock::now(); }
-
-  gst_status round() {
-    const size_t nj = active_.size();
-    for (Job* j : active_) decide(j);
-    // launch lists: for each action type, job slots + exclusive prefix of items
-    std::vector<uint32_t> lists;
-    struct L {
-      size_t jobs_off = 0, pre_off = 0;
-      int n = 0;
-      uint32_t total = 0;
-    };
-    auto build = [&](Action a, auto items_of) {
-      L l;
-      std::vector<uint32_t> js, pre;
-      uint32_t tot = 0;
-      for (size_t i = 0; i < nj; i++) {
-        Job* j = active_[i];
-        if (j->act != a) continue;
-        uint32_t n = items_of(j);
-        js.push_back((uint32_t)i);
-        pre.push_back(tot);
-        tot += n;
-      }
-      pre.push_back(tot);
-      l.n = (int)js.size();
-      l.total = tot;
-      l.jobs_off = lists.size();
-      lists.insert(lists.end(), js.begin(), js.end());
-      l.pre_off = lists.size();
-      lists.insert(lists.end(), pre.begin(), pre.end());
-      return l;
-    };
-    L lw = build(A_WORK, [](Job* j) { return j->qd.n_in; });
-    L ls = build(A_SPLIT, [](Job* j) { return j->qd.n_far; });
-    L lss = build(A_SSEED, [](Job* j) { return (uint32_t)j->members.size(); });
-    L lds = build(A_DSEED, [](Job* j) { return (uint32_t)j->members.size(); });
-    L lt = build(A_TOUR, [](Job*) { return 1u; });
-    L le = build(A_EXTRACT, [](Job*) { return 1u; });
-    gst_status st = ensure_buffers(nj, lists.size());
-    if (st != GST_OK) return st;
-    for (size_t i = 0; i < nj; i++) {
-      active_[i]->qd.ctl = d_ctl_ + i;
-      h_qd_[i] = active_[i]->qd;
-      h_ctl_[i] = active_[i]->ctl;
-    }
-    memcpy(h_lists_, lists.data(), lists.size() * 4);
-    CK(cudaMemcpyAsync(d_qd_, h_qd_, nj * sizeof(QDev), cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(d_ctl_, h_ctl_, nj * sizeof(QCtl), cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(d_lists_, h_lists_, lists.size() * 4, cudaMemcpyHostToDevice, stream_));
-    GraphDev gd{g_->d_beg, g_->d_adj, g_->V};
-    const uint32_t* D = d_lists_;
-    auto grid_for = [&](uint64_t threads) {
-      uint64_t b = (threads + 255) / 256;
-      uint64_t maxb = (uint64_t)g_->num_sms * 8;
-      return (unsigned)std::max<uint64_t>(1, std::min(b, maxb));
-    };
-    if (lss.n)
-      k_sssp_seed<<<grid_for(lss.total), 256, 0, stream_>>>(d_qd_, D + lss.jobs_off, D + lss.pre_off, lss.n,
-                                                           lss.total);
-    if (lds.n)
-      k_dp_seed<<<grid_for(lds.total), 256, 0, stream_>>>(d_qd_, D + lds.jobs_off, D + lds.pre_off, lds.n,
-                                                         lds.total);
-    if (ls.n && ls.total)
-      k_split<<<grid_for(ls.total), 256, 0, stream_>>>(d_qd_, D + ls.jobs_off, D + ls.pre_off, ls.n, ls.total);
-    if (lw.n && lw.total)
-      k_work<<<grid_for((uint64_t)lw.total * 32), 256, 0, stream_>>>(d_qd_, D + lw.jobs_off, D + lw.pre_off,
-                                                                     lw.n, lw.total, gd);
-    if (lt.n) k_tour<<<lt.n, 256, 0, stream_>>>(d_qd_, D + lt.jobs_off);
-    if (le.n) k_extract<<<(le.n + 63) / 64, 64, 0, stream_>>>(d_qd_, D + le.jobs_off, le.n, gd);
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(h_ctl_, d_ctl_, nj * sizeof(QCtl), cudaMemcpyDeviceToHost, stream_));
-    // tree edges of extracted jobs
-    CK(cudaStreamSynchronize(stream_));
-    for (size_t i = 0; i < nj; i++) active_[i]->ctl = h_ctl_[i];
-    for (size_t i = 0; i < nj; i++) {
-      Job* j = active_[i];
-      if (j->act == A_EXTRACT && j->ctl.status == 0 && j->ctl.best_full != INF64) {
-        uint32_t ne = std::min(j->ctl.n_edges, j->qd.max_edges);
+  template <class DoneFn>
+  gst_status retire(DoneFn&& on_done) {
+    std::vector<Job*> fin;
+    for (uint32_t s = 0; s < nslots_hi_; s++) {
+      Job* j = slots_[s];
+      if (!j || !h_ctl_[s].done) continue;
+      j->ctl = h_ctl_[s];
+      j->status = (gst_status)j->ctl.final_status;
+      if (j->status == GST_OK) {
+        j->cost = (int32_t)(j->ctl.best_full >> 32);
+        j->root = j->ctl.root;
+        uint32_t ne = std::min(j->ctl.n_edges, max_edges_dev_);
         j->edges.resize((size_t)ne * 3);
         if (ne) CK(cudaMemcpyAsync(j->edges.data(), j->qd.out_edges, (size_t)ne * 12, cudaMemcpyDeviceToHost, stream_));
       }
+      fin.push_back(j);
     }
+    if (fin.empty()) return GST_OK;
     CK(cudaStreamSynchronize(stream_));
-    for (Job* j : active_) {
-      absorb(j);
-      if (j->st == J_DONE && j->t_done.time_since_epoch().count() == 0) finish_timestamps(j);
+    auto now = std::chrono::steady_clock::now();
+    for (Job* j : fin) {
+      // free the slot: a zeroed descriptor is J_FREE for k_control
+      QDev z;
+      memset(&z, 0, sizeof(z));
+      CK(cudaMemcpyAsync(d_qd_ + j->slot, &z, sizeof(QDev), cudaMemcpyHostToDevice, stream_));
+      slots_[j->slot] = nullptr;
+      n_used_--;
+      free_job(j);
+      j->t_done = now;
+      j->done = true;
+      on_done(j);
     }
+    while (nslots_hi_ > 0 && !slots_[nslots_hi_ - 1]) nslots_hi_--;
     return GST_OK;
   }
 
   gst_graph* g_;
   cudaStream_t stream_ = nullptr;
-  std::vector<Job*> active_, finished_;
+  std::vector<Job*> slots_;
+  uint32_t n_used_ = 0, nslots_hi_ = 0, max_slots_ = MAX_SLOTS - 1;
   QDev* d_qd_ = nullptr;
   QCtl* d_ctl_ = nullptr;
-  uint32_t* d_lists_ = nullptr;
-  QDev* h_qd_ = nullptr;
+  RoundDesc* d_rd_ = nullptr;
+  uint32_t* d_pre_ = nullptr;
   QCtl* h_ctl_ = nullptr;
-  uint32_t* h_lists_ = nullptr;
-  size_t cap_jobs_ = 0, cap_lists_ = 0;
-  uint32_t delta_sssp_ = 4, delta_dp_ = 2, max_edges_dev_ = 1u << 16;
+  RoundDesc* h_rd_ = nullptr;
+  QDev* h_qd_ = nullptr;
+  uint32_t delta_sssp_ = 8, delta_dp_ = 2, max_edges_dev_ = 1u << 16;
+  uint32_t cap_num_ = 1, cap_den_ = 2, rounds_per_sync_ = 6;
+  cudaEvent_t ev_[2 + 2 * 64] = {};
+  unsigned light_grid_ = 148 * 4, heavy_grid_ = 148 * 2;
+  double last_call_ms_ = 0;
 };
 
 // Copy a finished job into a caller result.
@@ -537,9 +414,8 @@ gst_status fill_result(Job* j, gst_result* r) {
   r->cost = j->status == GST_OK ? j->cost : -1;
   r->root = j->root;
   for (int i = 0; i < GST_NSTATS; i++) r->stats[i] = j->ctl.stat[i];
-  r->stats[GST_STAT_ROUNDS] = j->rounds;
   r->stats[GST_STAT_TABLE_BYTES] = j->table_bytes;
-  r->device_ms = std::chrono::duration<double, std::milli>(j->t_done - j->t_admit).count();
+  r->latency_ms = std::chrono::duration<double, std::milli>(j->t_done - j->t_submit).count();
   gst_status st = j->status;
   if (st == GST_OK) {
     int32_t ne = (int32_t)(j->edges.size() / 3);
@@ -650,9 +526,31 @@ gst_status gst_groups_set(gst_graph* g, const uint64_t* grp_ptr, const uint32_t*
 
 void gst_graph_destroy(gst_graph* g) {
   if (!g) return;
+  if (g->runner) delete static_cast<Runner*>(g->runner);
   if (g->d_beg) cudaFree(g->d_beg);
   if (g->d_adj) cudaFree(g->d_adj);
   delete g;
+}
+
+uint64_t gst_kernel_launches(const gst_graph* g) { return g ? g->launches.load() : 0; }
+
+void gst_profile_enable(gst_graph* g, int on) {
+  if (g) g->profile = on != 0;
+}
+
+void gst_profile_read(const gst_graph* g, double* work_ms, uint64_t* work_launches, uint64_t* totals) {
+  if (!g) return;
+  if (work_ms) *work_ms = g->prof_work_ms;
+  if (work_launches) *work_launches = g->prof_work_launches;
+  if (totals)
+    for (int t = 0; t < GST_NSTATS; t++) totals[t] = g->prof_stats[t];
+}
+
+void gst_profile_reset(gst_graph* g) {
+  if (!g) return;
+  g->prof_work_ms = 0;
+  g->prof_work_launches = 0;
+  for (int t = 0; t < GST_NSTATS; t++) g->prof_stats[t] = 0;
 }
 
 uint32_t gst_graph_num_vertices(const gst_graph* g) { return g ? g->V : 0; }
@@ -673,9 +571,17 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
                            gst_result* results, int32_t* statuses, int max_concurrent) {
   if (!g || n < 0 || (n > 0 && (!groups || !ks || !Ds || !statuses))) return GST_BAD_INPUT;
   if (g->grp_ptr.empty()) return GST_BAD_INPUT;
-  Runner R(g);
-  gst_status st = R.init();
-  if (st != GST_OK) return st;
+  std::lock_guard<std::mutex> lock(g->mu);
+  if (!g->runner) {
+    Runner* nr = new Runner(g);
+    gst_status st = nr->init();
+    if (st != GST_OK) {
+      delete nr;
+      return st;
+    }
+    g->runner = nr;
+  }
+  Runner& R = *static_cast<Runner*>(g->runner);
   std::vector<Job> jobs(n);
   std::deque<Job*> pending;
   for (int i = 0; i < n; i++) {
@@ -686,7 +592,7 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
     j.res = results ? &results[i] : nullptr;
     if (j.k < 1 || j.k > KMAX) {
       statuses[i] = GST_BAD_INPUT;
-      j.st = J_DONE;
+      j.done = true;
       j.rejected = true;
       continue;
     }
@@ -699,34 +605,38 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
         j.res->cost = -1;
         j.res->n_edges = 0;
       }
-      j.st = J_DONE;
+      j.done = true;
       j.rejected = true;
       continue;
     }
     pending.push_back(&j);
   }
   const size_t maxc = max_concurrent > 0 ? (size_t)max_concurrent : (size_t)1 << 20;
-  gst_status rs = R.run([&](std::vector<Job*>& act) {
-    while (!pending.empty() && act.size() < maxc) {
-      Job* j = pending.front();
-      if (!R.admit(j)) {
-        if (act.empty()) {  // cannot fit even alone
-          j->status = GST_OOM;
-          j->st = J_DONE;
+  gst_status rs = R.run(
+      [&]() {
+        while (!pending.empty() && R.live() < maxc && R.has_free_slot()) {
+          Job* j = pending.front();
+          if (!R.admit(j)) {
+            if (R.live() == 0) {  // cannot fit even alone
+              j->status = GST_OOM;
+              j->done = true;
+              pending.pop_front();
+              continue;
+            }
+            break;
+          }
           pending.pop_front();
-          continue;
         }
-        break;
-      }
-      pending.pop_front();
-      act.push_back(j);
-    }
-  });
+      },
+      [&](Job*) {});
   if (rs != GST_OK) return rs;
   for (int i = 0; i < n; i++) {
     Job& j = jobs[i];
     if (j.rejected) continue;
     statuses[i] = fill_result(&j, j.res);
+    if (j.res) j.res->device_ms = R.last_call_ms();
+    if (g->profile)
+      for (int t = 0; t < GST_NSTATS; t++) g->prof_stats[t] += j.ctl.stat[t];
   }
   return GST_OK;
 }

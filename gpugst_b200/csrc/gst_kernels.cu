@@ -1,26 +1,29 @@
 // CUDA kernels of the gstb engine, sm_100a.
 //
 // Hot path of one query (the reference's DPBF_GPU, code/GPUGST/src/DPQ.cu:275-624,
-// and DPBF_gpu, code/D-GPUGST/src/DPQ.cu:149-269, re-designed):
-//   k_sssp_seed   group members -> distance items at 0        (DPQ.cu:359-368)
-//   k_work        one frontier round, warp per item:
-//                   distance item : multi-source relax of one (vertex, group)
-//                                   (replaces dis0_init_1, DPQ.cu:241-271)
+// and DPBF_gpu, code/D-GPUGST/src/DPQ.cu:149-269, re-designed).  Every round is
+//   k_control  one thread per query slot: advances the query's state machine
+//              (distance rounds -> tour tables -> DP seed -> DP rounds ->
+//              extraction) and writes the round's work description;
+//   k_light    warp tasks: near-far splits, seeds, tour tables, extraction and
+//              distance items (8 lanes per (vertex, group) item: multi-source
+//              relax, replacing dis0_init_1, DPQ.cu:241-271);
+//   k_heavy    warp per DP state:
 //                   DP item       : best update from complement / one-label
 //                                   completion, lower-bound prune, grow along
 //                                   the weight-sorted adjacency, merge with
 //                                   every disjoint subset at the vertex
 //                                   (replaces Relax, DPQ.cu:73-172 and
 //                                   D-GPUGST/src/DPQ.cu:62-126)
-//   k_split       near-far bucketing: moves far items whose cost entered the
-//                 new window to the near list
-//   k_tour        group-to-group distances and tour tables (host DP at
-//                 DPQ.cu:409-483, re-done on device by one CTA)
-//   k_dp_seed     cost-0 states of every subset of a member's group mask
-//                 (DPQ.cu:341-358)
-//   k_extract     follow parents from the best full state into a tree
-//                 (the reference's extraction, CPUNONHOP.h:390-432 /
-//                 CPUHOP.h:234-259, which its GPU path leaves commented out)
+//   split      near-far bucketing: far items whose cost entered the new
+//              window move to the near list
+//   tour       group-to-group distances and tour tables (host DP at
+//              DPQ.cu:409-483, re-done on device by one warp)
+//   seeds      members at distance 0 (DPQ.cu:359-368); cost-0 states of every
+//              subset of a member's group mask (DPQ.cu:341-358)
+//   extract    follow parents from the best full state into a tree (the
+//              reference's extraction, CPUNONHOP.h:390-432 / CPUHOP.h:234-259,
+//              which its GPU path leaves commented out)
 #include "gst_device.cuh"
 
 namespace gstb {
@@ -66,6 +69,40 @@ __device__ __forceinline__ void enqueue_warp(bool want, uint32_t s, uint32_t cos
   if (lane == 0 && cntm) atomicAdd(&q.ctl->stat[ST_ENQ], (unsigned long long)cntm);
 }
 
+// Enqueue for warps whose lanes may serve different queries (distance items
+// are processed by 8-lane groups).  Lanes are aggregated per (query, list)
+// with __match_any_sync.  `slot` identifies the query within the launch.
+__device__ __forceinline__ void enqueue_multi(bool want, uint32_t s, uint32_t cost, const QDev& q,
+                                              uint32_t* flags, uint32_t slot, uint32_t lane,
+                                              uint32_t& enq) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  bool nearq = cost < q.theta_hi;
+  bool take = false;
+  if (want) {
+    uint32_t bit = 1u << (2u * (s & 15u) + (nearq ? 0u : 1u));
+    uint32_t old = atomicOr(&flags[s >> 4], bit);
+    take = !(old & bit);
+  }
+  uint32_t key = take ? (slot * 2u + (nearq ? 0u : 1u)) : 0xFFFFFFFFu;
+  unsigned m = __match_any_sync(FULL, key);
+  uint32_t leader = __ffs(m) - 1;
+  uint32_t base = 0;
+  if (take && lane == leader) {
+    uint32_t* cnt = nearq ? &q.ctl->n_near : &q.ctl->n_far;
+    base = atomicAdd(cnt, (uint32_t)__popc(m));
+  }
+  base = __shfl_sync(FULL, base, leader);
+  if (take) {
+    uint32_t pos = base + __popc(m & ((1u << lane) - 1u));
+    uint32_t* buf = nearq ? q.qbuf[q.out_idx] : q.qbuf[q.far_idx];
+    if (pos < q.cap)
+      buf[pos] = s;
+    else
+      atomicExch(&q.ctl->overflow, 1u);
+    enq++;
+  }
+}
+
 // Load the capped group distances of vertex v into every lane's registers.
 __device__ __forceinline__ void load_dl(const QDev& q, uint32_t v, uint32_t (&dl)[KMAX],
                                         uint32_t& raw_sum_ok, uint32_t comp,
@@ -82,66 +119,6 @@ __device__ __forceinline__ void load_dl(const QDev& q, uint32_t v, uint32_t (&dl
       if (r[j] == INF32) raw_sum_ok = 0;
       raw_sum += r[j];
     }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Distance item: relax (v, group j) along arcs whose weight keeps the new
-// distance within the best known cost.
-// ---------------------------------------------------------------------------
-__device__ void sssp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t lane) {
-  const unsigned FULL = 0xFFFFFFFFu;
-  uint32_t v = s >> 3, j = s & 7u;
-  if (lane == 0) atomicAnd(&q.sflag[s >> 4], ~(1u << (2u * (s & 15u))));
-  __syncwarp();
-  uint32_t d = __shfl_sync(FULL, ld_cg(q.dist + s), 0);
-  uint32_t best = __shfl_sync(FULL, ld_cg(&q.ctl->best), 0);
-  if (d == INF32 || d > best) return;
-  // star bound: v joined to every group by its shortest paths (one-label
-  // completion of the empty tree at v, CPUNONHOP.h:684-699).  Not a valid
-  // bound under a hop limit, so only for unbounded queries.
-  if (q.D < 0) {
-    uint32_t dj = lane < (uint32_t)q.k ? ld_cg(q.dist + (size_t)v * 8 + lane) : 0u;
-    unsigned ok = __all_sync(FULL, dj != INF32);
-    unsigned long long sum = dj;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(FULL, sum, o);
-    if (ok && lane == 0 && sum < best) atomicMin(&q.ctl->best, (uint32_t)sum);
-  }
-  best = __shfl_sync(FULL, ld_cg(&q.ctl->best), 0);
-  if (d > best) return;
-  uint32_t lim = best - d;
-  uint32_t a0 = __ldg(g.beg + v), a1 = __ldg(g.beg + v + 1);
-  uint32_t scanned = 0, upd = 0;
-  for (uint32_t base = a0; base < a1; base += 32) {
-    uint32_t a = base + lane;
-    bool in = a < a1;
-    uint2 arc = in ? __ldg(g.adj + a) : make_uint2(0, 0xFFFFFFFFu);
-    bool over = arc.y > lim;
-    bool want = false;
-    uint32_t it = 0, nd = 0;
-    if (in && !over) {
-      scanned++;
-      nd = d + arc.y;
-      it = arc.x * 8u + j;
-      if (nd < ld_cg(q.dist + it)) {
-        uint32_t old = atomicMin(q.dist + it, nd);
-        want = nd < old;
-        upd += want;
-      }
-    }
-    enqueue_warp(want, it, nd, q, q.sflag, lane);
-    if (__any_sync(FULL, over)) break;  // adjacency is sorted by weight
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    scanned += __shfl_xor_sync(FULL, scanned, o);
-    upd += __shfl_xor_sync(FULL, upd, o);
-  }
-  if (lane == 0) {
-    atomicAdd(&q.ctl->stat[ST_SSSP], 1ull);
-    atomicAdd(&q.ctl->stat[ST_ARCS], (unsigned long long)scanned);
-    atomicAdd(&q.ctl->stat[ST_UPDATES], (unsigned long long)upd);
   }
 }
 
@@ -393,85 +370,192 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
   }
 }
 
-// Find the job owning flat work index `it` (prefix is exclusive, size njobs+1).
-__device__ __forceinline__ int find_job(const uint32_t* __restrict__ prefix, int njobs, uint32_t it) {
-  int lo = 0, hi = njobs;  // prefix[lo] <= it < prefix[hi]
+// Slot owning flat item `it` of task type t: largest s with pre[s] <= it.
+__device__ __forceinline__ uint32_t find_slot(const uint32_t* __restrict__ pre, int nslots, uint32_t it) {
+  int lo = 0, hi = nslots;  // pre[lo] <= it < pre[hi]
   while (hi - lo > 1) {
     int mid = (lo + hi) >> 1;
-    if (__ldg(prefix + mid) <= it)
+    if (__ldcg(pre + mid) <= it)
       lo = mid;
     else
       hi = mid;
   }
-  return lo;
+  return (uint32_t)lo;
 }
 
-__global__ void __launch_bounds__(256) k_work(const QDev* __restrict__ qd, const uint32_t* __restrict__ jobs,
-                                              const uint32_t* __restrict__ prefix, int njobs,
-                                              uint32_t total, GraphDev g) {
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t it = warp; it < total; it += nwarps) {
-    int j = find_job(prefix, njobs, it);
-    const QDev& q = qd[__ldg(jobs + j)];
-    uint32_t s = q.qbuf[q.in_idx][it - __ldg(prefix + j)];
-    if (q.phase == PH_SSSP)
-      sssp_item(q, g, s, lane);
-    else if (q.phase == PH_DP)
-      dp_item(q, g, s, lane);
-    else
-      hop_item(q, g, s, lane);
+// ---------------------------------------------------------------------------
+// Distance items: one warp task = 4 items, 8 lanes each.  The weight-sorted
+// adjacency usually leaves only a few arcs under the limit, so a full warp
+// per item would idle most lanes.  Counters are kept per lane group and
+// flushed when the group moves to another query (and at kernel end).
+// ---------------------------------------------------------------------------
+struct SsspCounters {
+  QCtl* cur = nullptr;
+  uint32_t items = 0, arcs = 0, upd = 0, enq = 0;
+};
+
+__device__ __forceinline__ void sssp_flush(SsspCounters& sc, uint32_t sl) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  uint32_t a = sc.arcs, u = sc.upd, e = sc.enq;
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(FULL, a, o);
+    u += __shfl_xor_sync(FULL, u, o);
+    e += __shfl_xor_sync(FULL, e, o);
+  }
+  if (sc.cur && sl == 0) {
+    if (sc.items) atomicAdd(&sc.cur->stat[ST_SSSP], (unsigned long long)sc.items);
+    if (a) atomicAdd(&sc.cur->stat[ST_ARCS], (unsigned long long)a);
+    if (u) atomicAdd(&sc.cur->stat[ST_UPDATES], (unsigned long long)u);
+    if (e) atomicAdd(&sc.cur->stat[ST_ENQ], (unsigned long long)e);
+  }
+  sc.items = sc.arcs = sc.upd = sc.enq = 0;
+}
+
+__device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restrict__ pre, int nslots,
+                          uint32_t total, uint32_t task, const GraphDev& g, uint32_t lane, SsspCounters& sc) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  const uint32_t sub = lane >> 3, sl = lane & 7u, gbase = lane & ~7u;
+  const uint32_t it = task * 4u + sub;
+  const bool valid = it < total;
+  const uint32_t slot = valid ? find_slot(pre, nslots, it) : 0u;
+  const QDev& q = qd[slot];
+  // flush the group's counters when it changes query (group-uniform decision)
+  bool change = valid && q.ctl != sc.cur;
+  if (__any_sync(FULL, change)) {
+    // lanes of groups that change flush; others keep accumulating
+    unsigned cm = __ballot_sync(FULL, change);
+    bool mine = (cm >> gbase) & 1u;
+    uint32_t a = sc.arcs, u = sc.upd, e = sc.enq;
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(FULL, a, o);
+      u += __shfl_xor_sync(FULL, u, o);
+      e += __shfl_xor_sync(FULL, e, o);
+    }
+    if (mine) {
+      if (sc.cur && sl == 0) {
+        if (sc.items) atomicAdd(&sc.cur->stat[ST_SSSP], (unsigned long long)sc.items);
+        if (a) atomicAdd(&sc.cur->stat[ST_ARCS], (unsigned long long)a);
+        if (u) atomicAdd(&sc.cur->stat[ST_UPDATES], (unsigned long long)u);
+        if (e) atomicAdd(&sc.cur->stat[ST_ENQ], (unsigned long long)e);
+      }
+      sc.items = sc.arcs = sc.upd = sc.enq = 0;
+      sc.cur = q.ctl;
+    }
+  }
+  const uint32_t s = valid ? q.qbuf[q.in_idx][it - __ldcg(pre + slot)] : 0u;
+  const uint32_t v = s >> 3, jg = s & 7u;
+  if (valid && sl == 0) atomicAnd(&q.sflag[s >> 4], ~(1u << (2u * (s & 15u))));
+  __syncwarp();
+  uint32_t d = __shfl_sync(FULL, valid ? ld_cg(q.dist + s) : INF32, gbase);
+  uint32_t best = __shfl_sync(FULL, valid ? ld_cg(&q.ctl->best) : 0u, gbase);
+  bool active = valid && d != INF32 && d <= best;
+  // star bound at v (unbounded queries only): v joined to every group by
+  // shortest paths, a feasible tree (one-label completion, CPUNONHOP.h:684-699)
+  {
+    bool lanev = active && q.D < 0 && sl < (uint32_t)q.k;
+    uint32_t dj = lanev ? ld_cg(q.dist + (size_t)v * 8 + sl) : 0u;
+    unsigned bad = __ballot_sync(FULL, lanev && dj == INF32);
+    unsigned long long sum = dj;
+    sum += __shfl_xor_sync(FULL, sum, 4);
+    sum += __shfl_xor_sync(FULL, sum, 2);
+    sum += __shfl_xor_sync(FULL, sum, 1);
+    if (active && q.D < 0 && sl == 0 && ((bad >> gbase) & 0xFFu) == 0 && sum < best)
+      atomicMin(&q.ctl->best, (uint32_t)sum);
+  }
+  best = __shfl_sync(FULL, valid ? ld_cg(&q.ctl->best) : 0u, gbase);
+  // distances beyond cap(best) cannot lower a bound below best: skip them
+  const uint32_t capb = valid ? (uint32_t)((unsigned long long)best * q.cap_num / q.cap_den) : 0u;
+  active = active && d <= capb;
+  const uint32_t lim = active ? capb - d : 0u;
+  const uint32_t a0 = active ? __ldg(g.beg + v) : 0u, a1 = active ? __ldg(g.beg + v + 1) : 0u;
+  if (active && sl == 0) sc.items++;
+  bool done = !active;
+  for (uint32_t off = 0;; off += 8) {
+    bool more = !done && a0 + off < a1;
+    if (!__any_sync(FULL, more)) break;
+    uint32_t a = a0 + off + sl;
+    bool in = more && a < a1;
+    uint2 arc = in ? __ldg(g.adj + a) : make_uint2(0, 0xFFFFFFFFu);
+    bool over = in && arc.y > lim;
+    bool want = false;
+    uint32_t t = 0, nd = 0;
+    if (in && !over) {
+      sc.arcs++;
+      nd = d + arc.y;
+      t = arc.x * 8u + jg;
+      if (nd < ld_cg(q.dist + t)) {
+        uint32_t old = atomicMin(q.dist + t, nd);
+        want = nd < old;
+        sc.upd += want;
+      }
+    }
+    enqueue_multi(want, t, nd, q, q.sflag, slot, lane, sc.enq);
+    unsigned stop = __ballot_sync(FULL, over || (more && a + 1 >= a1));
+    if ((stop >> gbase) & 0xFFu) done = true;  // sorted by weight: the rest is heavier
   }
 }
 
-// Near-far split: far items whose cost is in [theta_lo, theta_hi) move to the
-// near list; costs above stay; costs below theta_lo were already expanded at
-// that cost (every new cost is >= the cost of the item that produced it).
-__global__ void __launch_bounds__(256) k_split(const QDev* __restrict__ qd, const uint32_t* __restrict__ jobs,
-                                               const uint32_t* __restrict__ prefix, int njobs,
-                                               uint32_t total) {
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < total; it += stride) {
-    int j = find_job(prefix, njobs, it);
-    const QDev& q = qd[__ldg(jobs + j)];
-    uint32_t s = q.qbuf[q.far_idx][it - __ldg(prefix + j)];
-    uint32_t* flags = q.phase == PH_SSSP ? q.sflag : q.dflag;
-    uint32_t cost = q.phase == PH_SSSP ? ld_cg(q.dist + s) : (uint32_t)(ld_cg(q.table + s) >> 32);
-    uint32_t best = ld_cg(&q.ctl->best);
-    uint32_t sh = 2u * (s & 15u);
-    if (cost < q.theta_lo || cost == INF32 || cost > best) {
-      atomicAnd(&flags[s >> 4], ~(2u << sh));
-    } else if (cost < q.theta_hi) {
-      atomicAnd(&flags[s >> 4], ~(2u << sh));
-      uint32_t old = atomicOr(&flags[s >> 4], 1u << sh);
-      if (!(old & (1u << sh))) {
-        uint32_t pos = atomicAdd(&q.ctl->n_near, 1u);
-        if (pos < q.cap)
-          q.qbuf[q.out_idx][pos] = s;
-        else
-          atomicExch(&q.ctl->overflow, 1u);
-      }
-    } else {
-      uint32_t pos = atomicAdd(&q.ctl->n_far2, 1u);
+// Near-far split of one far item: cost in [theta_lo, theta_hi) -> near list;
+// above -> far-out list; below theta_lo it was already expanded at that cost
+// (every new cost is >= the cost of the item that produced it) -> dropped.
+__device__ void split_item(const QDev& q, uint32_t s) {
+  uint32_t* flags = q.phase == PH_SSSP ? q.sflag : q.dflag;
+  uint32_t cost = q.phase == PH_SSSP ? ld_cg(q.dist + s) : (uint32_t)(ld_cg(q.table + s) >> 32);
+  uint32_t best = ld_cg(&q.ctl->best);
+  uint32_t sh = 2u * (s & 15u);
+  if (cost < q.theta_lo || cost == INF32 || cost > best) {
+    atomicAnd(&flags[s >> 4], ~(2u << sh));
+  } else if (cost < q.theta_hi) {
+    atomicAnd(&flags[s >> 4], ~(2u << sh));
+    uint32_t old = atomicOr(&flags[s >> 4], 1u << sh);
+    if (!(old & (1u << sh))) {
+      uint32_t pos = atomicAdd(&q.ctl->n_near, 1u);
       if (pos < q.cap)
-        q.qbuf[q.far2_idx][pos] = s;
+        q.qbuf[q.out_idx][pos] = s;
       else
         atomicExch(&q.ctl->overflow, 1u);
     }
+  } else {
+    uint32_t pos = atomicAdd(&q.ctl->n_far2, 1u);
+    if (pos < q.cap)
+      q.qbuf[q.far2_idx][pos] = s;
+    else
+      atomicExch(&q.ctl->overflow, 1u);
   }
 }
 
-// Members -> distance items at distance 0, all in the first near list.
-__global__ void k_sssp_seed(const QDev* __restrict__ qd, const uint32_t* __restrict__ jobs,
-                            const uint32_t* __restrict__ prefix, int njobs, uint32_t total) {
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < total; it += stride) {
-    int j = find_job(prefix, njobs, it);
-    const QDev& q = qd[__ldg(jobs + j)];
-    uint32_t s = __ldg(q.members + (it - __ldg(prefix + j)));
-    q.dist[s] = 0;
-    uint32_t old = atomicOr(&q.sflag[s >> 4], 1u << (2u * (s & 15u)));
+// Member item v*8+j -> distance 0, first near list.
+__device__ void sseed_item(const QDev& q, uint32_t s) {
+  q.dist[s] = 0;
+  uint32_t old = atomicOr(&q.sflag[s >> 4], 1u << (2u * (s & 15u)));
+  if (!(old & (1u << (2u * (s & 15u))))) {
+    uint32_t pos = atomicAdd(&q.ctl->n_near, 1u);
+    if (pos < q.cap)
+      q.qbuf[q.out_idx][pos] = s;
+    else
+      atomicExch(&q.ctl->overflow, 1u);
+  }
+}
+
+// Cost-0 states: every non-empty subset of a member's mask (DPQ.cu:341-358).
+// The member item of the lowest group bit of the mask does the seeding.
+__device__ void dseed_item(const QDev& q, uint32_t item) {
+  uint32_t v = item >> 3, gi = item & 7u;
+  uint32_t m = 0;
+  for (int t = 0; t < q.k; t++)
+    if (q.dist[(size_t)v * 8 + t] == 0) m |= 1u << t;
+  if (m == 0 || (uint32_t)(__ffs(m) - 1) != gi) return;
+  for (uint32_t sub = m; sub; sub = (sub - 1u) & m) {
+    uint32_t s = q.phase == PH_HOP ? ((v << q.k) | sub) * (uint32_t)q.nd : ((v << q.k) | sub);
+    q.table[s] = pack(0u, 0u);
+    if (sub == (uint32_t)q.full) {  // v is in every query group: a cost-0 tree
+      atomicMin(&q.ctl->best, 0u);
+      atomicMin(&q.ctl->best_full, q.phase == PH_HOP ? (unsigned long long)(v * 8u) : (unsigned long long)v);
+      continue;
+    }
+    uint32_t old = atomicOr(&q.dflag[s >> 4], 1u << (2u * (s & 15u)));
     if (!(old & (1u << (2u * (s & 15u))))) {
       uint32_t pos = atomicAdd(&q.ctl->n_near, 1u);
       if (pos < q.cap)
@@ -482,87 +566,49 @@ __global__ void k_sssp_seed(const QDev* __restrict__ qd, const uint32_t* __restr
   }
 }
 
-// Cost-0 states: every non-empty subset of a member's mask (DPQ.cu:341-358).
-// The member item of the lowest group bit of the mask does the seeding.
-__global__ void k_dp_seed(const QDev* __restrict__ qd, const uint32_t* __restrict__ jobs,
-                          const uint32_t* __restrict__ prefix, int njobs, uint32_t total) {
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < total; it += stride) {
-    int j = find_job(prefix, njobs, it);
-    const QDev& q = qd[__ldg(jobs + j)];
-    uint32_t item = __ldg(q.members + (it - __ldg(prefix + j)));
-    uint32_t v = item >> 3, gi = item & 7u;
-    uint32_t m = 0;
-    for (int t = 0; t < q.k; t++)
-      if (q.dist[(size_t)v * 8 + t] == 0) m |= 1u << t;
-    if (m == 0 || (uint32_t)(__ffs(m) - 1) != gi) continue;
-    for (uint32_t sub = m; sub; sub = (sub - 1u) & m) {
-      uint32_t s = q.phase == PH_HOP ? ((v << q.k) | sub) * (uint32_t)q.nd : ((v << q.k) | sub);
-      q.table[s] = pack(0u, 0u);
-      if (sub == (uint32_t)q.full) {  // v is in every query group: a cost-0 tree
-        atomicMin(&q.ctl->best, 0u);
-        atomicMin(&q.ctl->best_full, q.phase == PH_HOP ? (unsigned long long)(v * 8u) : (unsigned long long)v);
-        continue;
-      }
-      uint32_t old = atomicOr(&q.dflag[s >> 4], 1u << (2u * (s & 15u)));
-      if (!(old & (1u << (2u * (s & 15u))))) {
-        uint32_t pos = atomicAdd(&q.ctl->n_near, 1u);
-        if (pos < q.cap)
-          q.qbuf[q.out_idx][pos] = s;
-        else
-          atomicExch(&q.ctl->overflow, 1u);
-      }
-    }
-  }
-}
-
-// One CTA per query: group-to-group distances gd[i][j] = min over members of
+// One warp per query: group-to-group distances gd[i][j] = min over members of
 // group i of the (capped) distance to group j, then the tour tables
 //   P[i][S][j]  cheapest visiting order of S starting at i, ending at j
 //   T2[i][S]    min_j P[i][S][j]
 // (replaces the host DP of DPQ.cu:409-483 / AllPaths, CPUNONHOP.h:269-386).
-__global__ void __launch_bounds__(256) k_tour(const QDev* __restrict__ qd, const uint32_t* __restrict__ jobs) {
-  const QDev& q = qd[jobs[blockIdx.x]];
+__device__ void tour_warp(const QDev& q, uint32_t lane) {
   const int k = q.k;
   const uint32_t K2 = 1u << k;
-  __shared__ uint32_t gd[KMAX][KMAX];
-  for (int t = threadIdx.x; t < KMAX * KMAX; t += blockDim.x) gd[t / KMAX][t % KMAX] = BIG;
-  __syncthreads();
-  for (uint32_t t = threadIdx.x; t < q.n_members; t += blockDim.x) {
-    uint32_t item = q.members[t];
-    uint32_t v = item >> 3, i = item & 7u;
-    for (int j = 0; j < k; j++) {
-      uint32_t dj = min(q.dist[(size_t)v * 8 + j], q.cap1);
-      atomicMin(&gd[i][j], dj);
-    }
-  }
-  __syncthreads();
   uint32_t* P = q.tour;
   uint32_t* T2 = q.tour + (size_t)k * K2 * k;
+  uint32_t* gd = T2 + (size_t)k * K2;  // [8][8]
+  for (uint32_t t = lane; t < 64; t += 32) gd[t] = BIG;
+  __syncwarp();
+  for (uint32_t t = lane; t < q.n_members; t += 32) {
+    uint32_t item = q.members[t];
+    uint32_t v = item >> 3, i = item & 7u;
+    for (int j = 0; j < k; j++) atomicMin(&gd[i * 8 + j], min(q.dist[(size_t)v * 8 + j], q.cap1));
+  }
+  __syncwarp();
   const uint32_t nP = (uint32_t)k * K2 * (uint32_t)k;
-  for (uint32_t t = threadIdx.x; t < nP; t += blockDim.x) P[t] = BIG;
-  __syncthreads();
-  for (int i = threadIdx.x; i < k; i += blockDim.x) P[((size_t)i * K2 + (1u << i)) * k + i] = 0;
-  __syncthreads();
+  for (uint32_t t = lane; t < nP; t += 32) P[t] = BIG;
+  __syncwarp();
+  for (uint32_t i = lane; i < (uint32_t)k; i += 32) P[((size_t)i * K2 + (1u << i)) * k + i] = 0;
+  __syncwarp();
   for (int size = 2; size <= k; size++) {
-    // entries (i, S, l) with |S| = size, i in S, l in S \ {i}
-    for (uint32_t t = threadIdx.x; t < nP; t += blockDim.x) {
+    for (uint32_t t = lane; t < nP; t += 32) {
       uint32_t l = t % k, S = (t / k) % K2, i = t / (k * K2);
       if ((uint32_t)__popc(S) != (uint32_t)size || !(S >> i & 1u) || !(S >> l & 1u) || l == i) continue;
       uint32_t Sp = S ^ (1u << l);
       uint32_t bestv = BIG;
       for (int jj = 0; jj < k; jj++)
-        if (Sp >> jj & 1u) bestv = min(bestv, sat_add(P[((size_t)i * K2 + Sp) * k + jj], gd[jj][l]));
+        if (Sp >> jj & 1u) bestv = min(bestv, sat_add(P[((size_t)i * K2 + Sp) * k + jj], __ldcg(&gd[jj * 8 + l])));
       P[t] = bestv;
     }
-    __syncthreads();
+    __syncwarp();
   }
-  for (uint32_t t = threadIdx.x; t < (uint32_t)k * K2; t += blockDim.x) {
+  for (uint32_t t = lane; t < (uint32_t)k * K2; t += 32) {
     uint32_t i = t / K2, S = t % K2;
     uint32_t m = BIG;
     for (int l = 0; l < k; l++) m = min(m, P[((size_t)i * K2 + S) * k + l]);
     T2[t] = m;
   }
+  __syncwarp();
 }
 
 // Weight of arc (a -> b): linear scan of a's weight-sorted adjacency.
@@ -574,13 +620,9 @@ __device__ uint32_t arc_weight(const GraphDev& g, uint32_t a, uint32_t b) {
   return INF32;
 }
 
-// One thread per query: follow parent words from the best full state,
-// emitting (u, v, w) edges; qbuf[0] serves as the explicit stack.
-__global__ void k_extract(const QDev* __restrict__ qd, const uint32_t* __restrict__ jobs, int njobs,
-                          GraphDev g) {
-  int jj = blockIdx.x * blockDim.x + threadIdx.x;
-  if (jj >= njobs) return;
-  const QDev& q = qd[jobs[jj]];
+// Follow parent words from the best full state, emitting (u, v, w) edges;
+// qbuf[0] serves as the explicit stack.  Run by one thread.
+__device__ void extract_one(const QDev& q, const GraphDev& g) {
   QCtl* ctl = q.ctl;
   unsigned long long bf = ctl->best_full;
   if (bf == INF64) {
@@ -597,10 +639,8 @@ __global__ void k_extract(const QDev* __restrict__ qd, const uint32_t* __restric
   uint32_t sp = 0;
   uint32_t full = (uint32_t)q.full;
   stack[sp++] = hop ? ((root << k) | full) * (uint32_t)nd + rd : ((root << k) | full);
-  uint32_t ne = 0;
-  uint32_t steps = 0;
+  uint32_t ne = 0, steps = 0, status = 0;
   const uint32_t max_steps = 4u * g.V + 64u;
-  uint32_t status = 0;
   while (sp > 0) {
     if (++steps > max_steps || sp + 2 > q.cap) {
       status = 2;
@@ -656,6 +696,271 @@ __global__ void k_extract(const QDev* __restrict__ qd, const uint32_t* __restric
   ctl->status = status;
   ctl->n_edges = ne;
   ctl->root = root;
+}
+
+// ---------------------------------------------------------------------------
+// Control: one thread per slot.  Absorbs the previous round's counters,
+// decides this round's action, and publishes per-type item counts as
+// exclusive prefix sums over slots (pre[t][0..nslots]).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void absorb(QDev& q, QCtl& c) {
+  if (c.overflow) {
+    q.st = J_DONE;
+    c.final_status = 6;  // GST_QUEUE_OVERFLOW
+    c.done = 1;
+    return;
+  }
+  int t;
+  switch (q.act) {
+    case A_SSEED:
+      t = q.in_idx; q.in_idx = q.out_idx; q.out_idx = t;
+      q.n_in = c.n_near;
+      q.n_far = 0;
+      q.st = J_SSSP;
+      break;
+    case A_WORK:
+      t = q.in_idx; q.in_idx = q.out_idx; q.out_idx = t;
+      q.n_in = c.n_near;
+      q.n_far = c.n_far;
+      break;
+    case A_SPLIT:
+      t = q.in_idx; q.in_idx = q.out_idx; q.out_idx = t;
+      t = q.far_idx; q.far_idx = q.far2_idx; q.far2_idx = t;
+      q.n_in = c.n_near;
+      q.n_far = c.n_far2;
+      break;
+    case A_TOUR:
+      q.st = J_DPSEED;
+      break;
+    case A_DSEED:
+      t = q.in_idx; q.in_idx = q.out_idx; q.out_idx = t;
+      q.n_in = c.n_near;
+      q.n_far = 0;
+      q.st = J_DP;
+      break;
+    case A_EXTRACT:
+      q.st = J_DONE;
+      c.final_status = c.status == 1 ? 1u : (c.status != 0 ? 8u : 0u);  // NO_SOLUTION / INTERNAL / OK
+      c.done = 1;
+      break;
+    default:
+      break;
+  }
+  if (q.act != A_NONE) c.stat[ST_ROUNDS]++;
+  q.act = A_NONE;
+}
+
+__device__ __forceinline__ void decide(QDev& q, QCtl& c) {
+  for (int guard = 0; guard < 8; guard++) {
+    switch (q.st) {
+      case J_INIT:
+        q.phase = PH_SSSP;
+        q.theta_lo = 0;
+        q.theta_hi = q.delta_sssp;
+        q.delta = q.delta_sssp;
+        c.n_near = 0;
+        q.act = A_SSEED;
+        return;
+      case J_SSSP:
+      case J_DP: {
+        if (q.n_in > 0) {
+          c.n_near = 0;
+          c.n_far = q.n_far;
+          q.act = A_WORK;
+          return;
+        }
+        uint32_t next_lo = q.theta_hi;
+        // distance rounds only matter up to cap(best); DP rounds up to best
+        unsigned long long limit = c.best;
+        if (q.st == J_SSSP && c.best != INF32) limit = (unsigned long long)c.best * q.cap_num / q.cap_den;
+        bool exhausted = q.n_far == 0 || next_lo > limit;
+        if (!exhausted) {
+          q.theta_lo = next_lo;
+          q.theta_hi = next_lo + q.delta;
+          c.n_near = 0;
+          c.n_far2 = 0;
+          q.act = A_SPLIT;
+          return;
+        }
+        if (q.st == J_SSSP) {
+          // every distance below theta_hi is exact and every distance <=
+          // cap(best) was discovered; unknown ones are >= min(theta_hi, cap+1)
+          unsigned long long b1 = c.best == INF32 ? (unsigned long long)INF32 : limit + 1;
+          unsigned long long cap1 = q.n_far == 0 ? b1 : (q.theta_hi < b1 ? q.theta_hi : b1);
+          q.cap1 = (uint32_t)(cap1 < BIG ? cap1 : BIG);
+          q.st = J_TOUR;
+          continue;
+        }
+        q.st = J_EXTRACT;
+        continue;
+      }
+      case J_TOUR:
+        q.act = A_TOUR;
+        return;
+      case J_DPSEED:
+        q.phase = q.D < 0 ? PH_DP : PH_HOP;
+        q.theta_lo = 0;
+        q.theta_hi = q.delta_dp;
+        q.delta = q.delta_dp;
+        q.n_in = 0;
+        q.n_far = 0;
+        c.n_near = 0;
+        c.n_far = 0;
+        q.act = A_DSEED;
+        return;
+      case J_EXTRACT:
+        q.act = A_EXTRACT;
+        return;
+      default:
+        q.act = A_NONE;
+        return;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* __restrict__ ctl, int nslots,
+                                                  RoundDesc* __restrict__ rd, uint32_t* __restrict__ pre) {
+  __shared__ uint32_t wsum[32][NT];
+  __shared__ uint32_t live_cnt;
+  const int tid = threadIdx.x;
+  const uint32_t lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) live_cnt = 0;
+  __syncthreads();
+  uint32_t cnt[NT];
+#pragma unroll
+  for (int t = 0; t < NT; t++) cnt[t] = 0;
+  if (tid < nslots) {
+    QDev q = qd[tid];
+    QCtl& c = ctl[tid];
+    if (q.st != J_FREE && q.st != J_DONE) {
+      absorb(q, c);
+      if (q.st != J_DONE) decide(q, c);
+      switch (q.act) {
+        case A_SSEED: cnt[T_SSEED] = q.n_members; break;
+        case A_DSEED: cnt[T_DSEED] = q.n_members; break;
+        case A_SPLIT: cnt[T_SPLIT] = q.n_far; break;
+        case A_TOUR: cnt[T_TOUR] = 1; break;
+        case A_EXTRACT: cnt[T_EXTRACT] = 1; break;
+        case A_WORK:
+          cnt[q.phase == PH_SSSP ? T_SSSP : (q.phase == PH_DP ? T_DP : T_HOP)] = q.n_in;
+          break;
+        default: break;
+      }
+      if (q.st != J_DONE) atomicAdd(&live_cnt, 1u);
+      qd[tid] = q;
+    }
+  }
+  // exclusive scan over slots, per task type
+  uint32_t incl[NT];
+#pragma unroll
+  for (int t = 0; t < NT; t++) {
+    uint32_t x = cnt[t];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+      if (lane >= (uint32_t)o) x += y;
+    }
+    incl[t] = x;
+    if (lane == 31) wsum[wid][t] = x;
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+      uint32_t x = lane < (blockDim.x >> 5) ? wsum[lane][t] : 0u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+      }
+      wsum[lane][t] = x;  // inclusive over warps
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int t = 0; t < NT; t++) {
+    uint32_t before = (wid ? wsum[wid - 1][t] : 0u) + incl[t] - cnt[t];
+    if (tid <= nslots) pre[t * (MAX_SLOTS + 1) + tid] = before;
+  }
+  if (tid == 0) {
+    const uint32_t per_task[NT] = {32, 32, 32, 1, 1, 4, 1, 1};
+    uint32_t off = 0;
+    for (int t = 0; t < NT; t++) {
+      uint32_t tot = wsum[(blockDim.x >> 5) - 1][t];
+      rd->items[t] = tot;
+      if (t == T_DP) {
+        rd->light_tasks = off;
+        off = 0;
+      }
+      rd->task_off[t] = off;
+      off += (tot + per_task[t] - 1) / per_task[t];
+    }
+    rd->task_off[NT] = off;
+    rd->heavy_tasks = off;
+    rd->n_live = live_cnt;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Light round kernel: warp tasks of types T_SPLIT .. T_SSSP.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_light(const QDev* __restrict__ qd, const RoundDesc* __restrict__ rd,
+                                               const uint32_t* __restrict__ pre, int nslots, GraphDev g) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t ntasks = __ldcg(&rd->light_tasks);
+  SsspCounters sc;
+  for (uint32_t task = warp; task < ntasks; task += nwarps) {
+    int t = 0;
+    while (t < T_SSSP && task >= __ldcg(&rd->task_off[t + 1])) t++;
+    const uint32_t local = task - __ldcg(&rd->task_off[t]);
+    const uint32_t* P = pre + t * (MAX_SLOTS + 1);
+    const uint32_t total = __ldcg(&rd->items[t]);
+    if (t == T_SSSP) {
+      sssp_task(qd, P, nslots, total, local, g, lane, sc);
+    } else if (t == T_TOUR) {
+      tour_warp(qd[find_slot(P, nslots, local)], lane);
+    } else if (t == T_EXTRACT) {
+      if (lane == 0) extract_one(qd[find_slot(P, nslots, local)], g);
+    } else {
+      uint32_t it = local * 32u + lane;
+      if (it < total) {
+        uint32_t slot = find_slot(P, nslots, it);
+        const QDev& q = qd[slot];
+        uint32_t idx = it - __ldcg(P + slot);
+        if (t == T_SPLIT)
+          split_item(q, q.qbuf[q.far_idx][idx]);
+        else if (t == T_SSEED)
+          sseed_item(q, __ldg(q.members + idx));
+        else
+          dseed_item(q, __ldg(q.members + idx));
+      }
+    }
+  }
+  sssp_flush(sc, lane & 7u);
+}
+
+// Heavy round kernel: one warp per DP state (unbounded, then hop-bounded).
+__global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, const RoundDesc* __restrict__ rd,
+                                               const uint32_t* __restrict__ pre, int nslots, GraphDev g) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t ntasks = __ldcg(&rd->heavy_tasks);
+  const uint32_t ndp = __ldcg(&rd->items[T_DP]);
+  for (uint32_t task = warp; task < ntasks; task += nwarps) {
+    const bool hop = task >= ndp;
+    const uint32_t it = hop ? task - ndp : task;
+    const uint32_t* P = pre + (hop ? T_HOP : T_DP) * (MAX_SLOTS + 1);
+    const uint32_t slot = find_slot(P, nslots, it);
+    const QDev& q = qd[slot];
+    const uint32_t s = q.qbuf[q.in_idx][it - __ldcg(P + slot)];
+    if (hop)
+      hop_item(q, g, s, lane);
+    else
+      dp_item(q, g, s, lane);
+  }
 }
 
 }  // namespace gstb

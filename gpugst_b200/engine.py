@@ -41,7 +41,8 @@ class GstError(RuntimeError):
 class _Result(ctypes.Structure):
     _fields_ = [("cost", ctypes.c_int32), ("root", ctypes.c_uint32), ("n_edges", ctypes.c_int32),
                 ("max_edges", ctypes.c_int32), ("edges", ctypes.POINTER(ctypes.c_uint32)),
-                ("stats", ctypes.c_uint64 * 8), ("device_ms", ctypes.c_double)]
+                ("stats", ctypes.c_uint64 * 8), ("device_ms", ctypes.c_double),
+                ("latency_ms", ctypes.c_double)]
 
 
 _lib = None
@@ -66,6 +67,14 @@ def lib():
         L.gst_graph_num_vertices.argtypes = [vp]
         L.gst_graph_num_arcs.restype = u64
         L.gst_graph_num_arcs.argtypes = [vp]
+        L.gst_kernel_launches.argtypes = [vp]
+        L.gst_kernel_launches.restype = u64
+        L.gst_profile_enable.argtypes = [vp, ctypes.c_int]
+        L.gst_profile_enable.restype = None
+        L.gst_profile_read.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(u64), vp]
+        L.gst_profile_read.restype = None
+        L.gst_profile_reset.argtypes = [vp]
+        L.gst_profile_reset.restype = None
         for name in ("gst_graph_create", "gst_groups_set", "gst_query", "gst_query_batch"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
@@ -84,6 +93,7 @@ class QueryResult:
     edges: np.ndarray  # (n, 3) uint32: u, v, w
     stats: dict = field(default_factory=dict)
     device_ms: float = 0.0
+    latency_ms: float = 0.0
 
     @property
     def ok(self) -> bool:
@@ -136,7 +146,23 @@ class Engine:
         n = min(max(r.n_edges, 0), r.max_edges)
         edges = buf[:3 * n].reshape(-1, 3).copy() if st in (GST_OK, GST_TRUNCATED) else np.zeros((0, 3), np.uint32)
         stats = {name: int(r.stats[i]) for i, name in enumerate(STAT_NAMES)}
-        return QueryResult(st, r.cost, r.root, edges, stats, r.device_ms)
+        return QueryResult(st, r.cost, r.root, edges, stats, r.device_ms, r.latency_ms)
+
+    def kernel_launches(self) -> int:
+        return int(lib().gst_kernel_launches(self._h))
+
+    def profile(self, on: bool = True):
+        lib().gst_profile_enable(self._h, 1 if on else 0)
+
+    def profile_reset(self):
+        lib().gst_profile_reset(self._h)
+
+    def profile_read(self):
+        ms = ctypes.c_double(0)
+        n = ctypes.c_uint64(0)
+        tot = np.zeros(8, dtype=np.uint64)
+        lib().gst_profile_read(self._h, ctypes.byref(ms), ctypes.byref(n), _ptr(tot))
+        return ms.value, n.value, {name: int(tot[i]) for i, name in enumerate(STAT_NAMES)}
 
     def query(self, groups, D: int = -1, max_edges: int = 4096) -> QueryResult:
         """One synchronous query (gst_query)."""

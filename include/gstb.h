@@ -77,7 +77,9 @@ typedef struct gst_result {
   int32_t max_edges;       /* capacity of `edges` in edges (caller sets) */
   uint32_t* edges;         /* caller buffer, 3*max_edges uint32: (u, v, w) triples */
   uint64_t stats[GST_NSTATS];
-  double device_ms;        /* device time of the query (CUDA events) */
+  double device_ms;        /* device time of the call that ran this query (CUDA
+                              events around all of that call's rounds) */
+  double latency_ms;       /* host time from submission to completion */
 } gst_result;
 
 /* Replaces toCSR (code/GPUGST/include/graph_v_of_v_idealID/csr_graph.hpp:39-128):
@@ -132,6 +134,16 @@ gst_status gst_serve_poll(gst_server* s, uint64_t* ids, int32_t* statuses, gst_r
 gst_status gst_serve_close(gst_server* s);
 
 const char* gst_status_string(gst_status st);
+
+/* Diagnostics (no reference counterpart).  Kernel launches issued by this
+ * graph's engine so far, and, when profiling is on, the accumulated device
+ * time and launch count of the round kernel (k_work) plus the summed
+ * GST_STAT_* counters of the finished queries. */
+uint64_t gst_kernel_launches(const gst_graph* g);
+void gst_profile_enable(gst_graph* g, int on);
+void gst_profile_read(const gst_graph* g, double* work_ms, uint64_t* work_launches,
+                      uint64_t stats_totals[GST_NSTATS]);
+void gst_profile_reset(gst_graph* g);
 
 #ifdef __cplusplus
 }
