@@ -12,6 +12,7 @@
 //   sflag  u32 [ceil(V*8/16)]      2 bits per distance item
 //   qbuf   u32 [4][cap]        near-in, near-out, far, far-out work lists of state ids
 //   tour   u32 [k][2^k][k] + [k][2^k] + [8][8]  tour tables P, T2 and group distances
+//   lbt    u16 [V][2^k]        lower bound of completing (v, X) to every group
 #pragma once
 #include <cstdint>
 
@@ -26,12 +27,12 @@ constexpr int KMAX = 8;
 constexpr int DMAX = 7;
 
 // Job state machine (advanced on the device by k_control once per round).
-enum JobState : int32_t { J_FREE = 0, J_INIT, J_SSSP, J_TOUR, J_DPSEED, J_DP, J_EXTRACT, J_DONE };
-enum Action : int32_t { A_NONE = 0, A_SSEED, A_WORK, A_SPLIT, A_TOUR, A_DSEED, A_EXTRACT };
+enum JobState : int32_t { J_FREE = 0, J_INIT, J_SSSP, J_TOUR, J_LB, J_DPSEED, J_DP, J_EXTRACT, J_DONE };
+enum Action : int32_t { A_NONE = 0, A_SSEED, A_WORK, A_SPLIT, A_TOUR, A_LB, A_DSEED, A_EXTRACT };
 
 // Task types of one round.  Light kernel: split, seeds, tour, extract and
-// distance items; heavy kernel: DP items.
-enum TaskType : int32_t { T_SPLIT = 0, T_SSEED, T_DSEED, T_TOUR, T_EXTRACT, T_SSSP, T_DP, T_HOP, NT };
+// distance items; heavy kernel: lower-bound tables and DP items.
+enum TaskType : int32_t { T_SPLIT = 0, T_SSEED, T_DSEED, T_TOUR, T_EXTRACT, T_SSSP, T_LB, T_DP, T_HOP, NT };
 constexpr int MAX_SLOTS = 1024;
 
 // Round-wide work description written by k_control.
@@ -86,10 +87,12 @@ struct QDev {
   uint32_t* sflag;
   uint32_t* qbuf[4];
   uint32_t* tour;
+  unsigned short* lbt;      // [V][2^k] lower bound per (vertex, uncovered set)
   const uint32_t* members;  // distance items v*8+j of every query-group member
   uint32_t* out_edges;      // extraction output (u, v, w) triples
   QCtl* ctl;
   uint32_t cap;
+  uint32_t nv;              // number of vertices
   uint32_t n_members;
   uint32_t max_edges;
   int32_t k, D, nd, full;

@@ -107,7 +107,7 @@ size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // Workspace layout of one query (see gst_device.cuh).
 struct Layout {
-  size_t table, dist, dflag, sflag, qbuf, tour, members, edges, total;
+  size_t table, dist, dflag, sflag, qbuf, tour, lbt, members, edges, total;
   uint32_t cap;
 };
 
@@ -126,6 +126,7 @@ Layout layout_for(const gst_graph* g, int k, int nd, size_t n_members, uint32_t 
   L.sflag = o; o = align_up(o + (((size_t)g->V * 8 + 15) / 16) * 4, 256);
   L.qbuf = o; o = align_up(o + 4 * cap * 4, 256);
   L.tour = o; o = align_up(o + ((size_t)k * (1u << k) * k + (size_t)k * (1u << k) + 64) * 4, 256);
+  L.lbt = o; o = align_up(o + (size_t)g->V * (1u << k) * 2, 256);
   L.members = o; o = align_up(o + std::max<size_t>(n_members, 1) * 4, 256);
   L.edges = o; o = align_up(o + (size_t)std::max<uint32_t>(max_edges, 1) * 12, 256);
   L.total = o;
@@ -151,8 +152,8 @@ class Runner {
     CK(cudaDeviceGetDefaultMemPool(&pool, g_->device));
     uint64_t thr = ~0ull;
     CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
-    delta_sssp_ = std::max(1u, env_u32("GSTB_DELTA_SSSP", 8));
-    delta_dp_ = std::max(1u, env_u32("GSTB_DELTA_DP", 2));
+    delta_sssp_ = std::max(1u, env_u32("GSTB_DELTA_SSSP", 16));
+    delta_dp_ = std::max(1u, env_u32("GSTB_DELTA_DP", 4));
     cap_num_ = std::max(1u, env_u32("GSTB_SSSP_CAP_NUM", 1));
     cap_den_ = std::max(1u, env_u32("GSTB_SSSP_CAP_DEN", 2));
     max_edges_dev_ = env_u32("GSTB_MAX_TREE_EDGES", 1u << 16);
@@ -256,6 +257,8 @@ class Runner {
     q.sflag = (uint32_t*)(j->mem + L.sflag);
     for (int b = 0; b < 4; b++) q.qbuf[b] = (uint32_t*)(j->mem + L.qbuf) + (size_t)b * L.cap;
     q.tour = (uint32_t*)(j->mem + L.tour);
+    q.lbt = (unsigned short*)(j->mem + L.lbt);
+    q.nv = g_->V;
     q.members = (const uint32_t*)(j->mem + L.members);
     q.out_edges = (uint32_t*)(j->mem + L.edges);
     q.ctl = d_ctl_ + slot;

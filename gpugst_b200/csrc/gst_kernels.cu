@@ -141,8 +141,6 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
     return;
   }
   const uint32_t comp = full ^ p;
-  const uint32_t* P = q.tour;
-  const uint32_t* T2 = q.tour + (size_t)k * K2 * k;
   uint32_t dl[KMAX], sum_ok;
   unsigned long long raw_sum;
   load_dl(q, v, dl, sum_ok, comp, raw_sum);
@@ -167,7 +165,8 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
   }
   __syncwarp();
   best = __shfl_sync(FULL, ld_cg(&q.ctl->best), 0);
-  uint32_t lbv = lower_bound_comp(dl, k, comp, P, T2);
+  const unsigned short* lbt = q.lbt;
+  uint32_t lbv = __ldg(lbt + ((size_t)v << k) + comp);
   if ((unsigned long long)c + lbv > best) return;
 
   uint32_t scanned = 0, upd = 0;
@@ -188,10 +187,7 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
         nc = c + arc.y;
         t = (arc.x << k) | p;
         if (nc < (uint32_t)(ld_cg(q.table + t) >> 32)) {
-          uint32_t dlu[KMAX], okb;
-          unsigned long long rs;
-          load_dl(q, arc.x, dlu, okb, comp, rs);
-          uint32_t lbu = lower_bound_comp(dlu, k, comp, P, T2);
+          uint32_t lbu = __ldg(lbt + ((size_t)arc.x << k) + comp);
           if ((unsigned long long)nc + lbu <= best) {
             unsigned long long old = atomicMin(q.table + t, pack(nc, PAR_GROW | v));
             want = (uint32_t)(old >> 32) > nc;
@@ -221,7 +217,7 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
           uint32_t qset = p | p2;
           // conditional tree merging: 3m <= 2 best (CPUNONHOP.h:941)
           if (3ull * m <= 2ull * best) {
-            uint32_t lbq = lower_bound_comp(dl, k, full ^ qset, P, T2);
+            uint32_t lbq = __ldg(lbt + ((size_t)v << k) + (full ^ qset));
             if (m + lbq <= best) {
               m32 = (uint32_t)m;
               t = (v << k) | qset;
@@ -274,13 +270,9 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
     return;
   }
   const uint32_t comp = full ^ p;
-  const uint32_t* P = q.tour;
-  const uint32_t* T2 = q.tour + (size_t)k * K2 * k;
-  uint32_t dl[KMAX], sum_ok;
-  unsigned long long raw_sum;
-  load_dl(q, v, dl, sum_ok, comp, raw_sum);
   if (lane == 0) atomicAdd(&q.ctl->stat[ST_EXPANDED], 1ull);
-  uint32_t lbv = lower_bound_comp(dl, k, comp, P, T2);
+  const unsigned short* lbt = q.lbt;
+  uint32_t lbv = __ldg(lbt + ((size_t)v << k) + comp);
   if ((unsigned long long)c + lbv > best) return;
   uint32_t scanned = 0, upd = 0;
   if (d < (uint32_t)D) {  // grow d -> d+1 (CPUHOP.h:192-206)
@@ -298,10 +290,7 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
         nc = c + arc.y;
         t = ((arc.x << k) | p) * (uint32_t)nd + d + 1;
         if (nc < (uint32_t)(ld_cg(q.table + t) >> 32)) {
-          uint32_t dlu[KMAX], okb;
-          unsigned long long rs;
-          load_dl(q, arc.x, dlu, okb, comp, rs);
-          uint32_t lbu = lower_bound_comp(dlu, k, comp, P, T2);
+          uint32_t lbu = __ldg(lbt + ((size_t)arc.x << k) + comp);
           if ((unsigned long long)nc + lbu <= best) {
             unsigned long long old = atomicMin(q.table + t, pack(nc, PAR_GROW | v));
             want = (uint32_t)(old >> 32) > nc;
@@ -343,7 +332,7 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
               atomicMin(&q.ctl->best, m32);
               atomicMin(&q.ctl->best_full, ((unsigned long long)m32 << 32) | (v * 8u + ndd));
             } else {
-              uint32_t lbq = lower_bound_comp(dl, k, full ^ qset, P, T2);
+              uint32_t lbq = __ldg(lbt + ((size_t)v << k) + (full ^ qset));
               if (m + lbq <= best) {
                 unsigned long long old = atomicMin(q.table + t, pack(m32, par));
                 want = (uint32_t)(old >> 32) > m32;
@@ -611,6 +600,29 @@ __device__ void tour_warp(const QDev& q, uint32_t lane) {
   __syncwarp();
 }
 
+// Lower-bound table of one vertex: lbt[v][X] = lower_bound_comp(d(v), X)
+// for every subset X, saturated to 16 bits (the per-vertex one_label_lb table
+// of the reference, DPQ.cu:174-224, with the tour bounds of
+// CPUNONHOP.h:436-496).  Saturation only lowers a bound, so it stays valid.
+__device__ void lbt_vertex(const QDev& q, uint32_t v) {
+  const int k = q.k;
+  const uint32_t K2 = 1u << k;
+  const uint32_t* P = q.tour;
+  const uint32_t* T2 = q.tour + (size_t)k * K2 * k;
+  const uint4* row = reinterpret_cast<const uint4*>(q.dist + (size_t)v * 8);
+  uint4 a = __ldcg(row), b = __ldcg(row + 1);
+  uint32_t r[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  uint32_t dl[KMAX];
+#pragma unroll
+  for (int j = 0; j < KMAX; j++) dl[j] = min(r[j], q.cap1);
+  unsigned short* out = q.lbt + ((size_t)v << k);
+  out[0] = 0;
+  for (uint32_t X = 1; X < K2; X++) {
+    uint32_t lb = lower_bound_comp(dl, k, X, P, T2);
+    out[X] = (unsigned short)min(lb, 65535u);
+  }
+}
+
 // Weight of arc (a -> b): linear scan of a's weight-sorted adjacency.
 __device__ uint32_t arc_weight(const GraphDev& g, uint32_t a, uint32_t b) {
   for (uint32_t x = g.beg[a]; x < g.beg[a + 1]; x++) {
@@ -730,6 +742,9 @@ __device__ __forceinline__ void absorb(QDev& q, QCtl& c) {
       q.n_far = c.n_far2;
       break;
     case A_TOUR:
+      q.st = J_LB;
+      break;
+    case A_LB:
       q.st = J_DPSEED;
       break;
     case A_DSEED:
@@ -797,6 +812,9 @@ __device__ __forceinline__ void decide(QDev& q, QCtl& c) {
       case J_TOUR:
         q.act = A_TOUR;
         return;
+      case J_LB:
+        q.act = A_LB;
+        return;
       case J_DPSEED:
         q.phase = q.D < 0 ? PH_DP : PH_HOP;
         q.theta_lo = 0;
@@ -840,6 +858,7 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
         case A_DSEED: cnt[T_DSEED] = q.n_members; break;
         case A_SPLIT: cnt[T_SPLIT] = q.n_far; break;
         case A_TOUR: cnt[T_TOUR] = 1; break;
+        case A_LB: cnt[T_LB] = q.nv; break;
         case A_EXTRACT: cnt[T_EXTRACT] = 1; break;
         case A_WORK:
           cnt[q.phase == PH_SSSP ? T_SSSP : (q.phase == PH_DP ? T_DP : T_HOP)] = q.n_in;
@@ -883,12 +902,12 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
     if (tid <= nslots) pre[t * (MAX_SLOTS + 1) + tid] = before;
   }
   if (tid == 0) {
-    const uint32_t per_task[NT] = {32, 32, 32, 1, 1, 4, 1, 1};
+    const uint32_t per_task[NT] = {32, 32, 32, 1, 1, 4, 32, 1, 1};
     uint32_t off = 0;
     for (int t = 0; t < NT; t++) {
       uint32_t tot = wsum[(blockDim.x >> 5) - 1][t];
       rd->items[t] = tot;
-      if (t == T_DP) {
+      if (t == T_LB) {
         rd->light_tasks = off;
         off = 0;
       }
@@ -941,17 +960,27 @@ __global__ void __launch_bounds__(256) k_light(const QDev* __restrict__ qd, cons
   sssp_flush(sc, lane & 7u);
 }
 
-// Heavy round kernel: one warp per DP state (unbounded, then hop-bounded).
+// Heavy round kernel: lower-bound table rows (one vertex per lane), then one
+// warp per DP state (unbounded, then hop-bounded).
 __global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, const RoundDesc* __restrict__ rd,
                                                const uint32_t* __restrict__ pre, int nslots, GraphDev g) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t ntasks = __ldcg(&rd->heavy_tasks);
-  const uint32_t ndp = __ldcg(&rd->items[T_DP]);
+  const uint32_t dp0 = __ldcg(&rd->task_off[T_DP]), hop0 = __ldcg(&rd->task_off[T_HOP]);
   for (uint32_t task = warp; task < ntasks; task += nwarps) {
-    const bool hop = task >= ndp;
-    const uint32_t it = hop ? task - ndp : task;
+    if (task < dp0) {  // lower-bound table rows, one vertex per lane
+      const uint32_t* P = pre + T_LB * (MAX_SLOTS + 1);
+      uint32_t it = task * 32u + lane;
+      if (it < __ldcg(&rd->items[T_LB])) {
+        uint32_t slot = find_slot(P, nslots, it);
+        lbt_vertex(qd[slot], it - __ldcg(P + slot));
+      }
+      continue;
+    }
+    const bool hop = task >= hop0;
+    const uint32_t it = hop ? task - hop0 : task - dp0;
     const uint32_t* P = pre + (hop ? T_HOP : T_DP) * (MAX_SLOTS + 1);
     const uint32_t slot = find_slot(P, nslots, it);
     const QDev& q = qd[slot];
