@@ -458,6 +458,7 @@ const char* gst_status_string(gst_status st) {
     case GST_INTERNAL: return "internal consistency check failed";
     case GST_BUSY: return "busy";
     case GST_NOT_FOUND: return "not found";
+    case GST_SCRATCH_TOO_SMALL: return "query workspace exceeds the static scratch";
   }
   return "unknown";
 }
@@ -645,3 +646,182 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free query (gst_query_noalloc).  One static device array holds
+// every buffer of a single query; its device address is looked up once per
+// device.  Uses the kernels of the regular path with a single slot.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[GST_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+std::mutex g_noalloc_mu;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+void* g_noalloc_base[NOALLOC_MAX_DEVICES] = {nullptr};
+
+// Restores the caller's current device on scope exit.
+struct DeviceGuard {
+  int prev = -1;
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+}  // namespace
+
+extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, int k, int D, gst_result* out) {
+  if (!g || !groups || k < 1 || k > KMAX || D > DMAX) return GST_BAD_INPUT;
+  if (g->grp_ptr.empty()) return GST_BAD_INPUT;
+  if (D < 0) D = -1;
+  const uint32_t ng = (uint32_t)(g->grp_ptr.size() - 1);
+  for (int i = 0; i < k; i++)
+    if (groups[i] >= ng) return GST_BAD_INPUT;
+  for (int a = 0; a < k; a++)
+    for (int b = a + 1; b < k; b++)
+      if (groups[a] == groups[b]) return GST_BAD_INPUT;
+  const int nd = D < 0 ? 1 : D + 1;
+  const uint32_t WT = (1u << k) * (uint32_t)nd;
+  if ((uint64_t)g->V * WT >= (1ull << 32)) return GST_BAD_INPUT;
+  uint64_t n_members = 0;
+  for (int i = 0; i < k; i++) {
+    uint64_t n = g->grp_ptr[groups[i] + 1] - g->grp_ptr[groups[i]];
+    if (n == 0) return GST_NO_SOLUTION;
+    n_members += n;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  DeviceGuard guard;
+  CK(cudaGetDevice(&guard.prev));
+  CK(cudaSetDevice(g->device));
+  if (g->device < 0 || g->device >= NOALLOC_MAX_DEVICES) return GST_BAD_INPUT;
+  if (!g_noalloc_base[g->device]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_base[g->device] = p;
+  }
+  char* base = static_cast<char*>(g_noalloc_base[g->device]);
+
+  // scratch = [QDev][QCtl][RoundDesc][pre: NT x (MAX_SLOTS+1)][workspace]
+  const uint32_t max_edges = 4096;
+  size_t o = 0;
+  const size_t o_qd = o;
+  o = align_up(o + sizeof(QDev), 256);
+  const size_t o_ctl = o;
+  o = align_up(o + sizeof(QCtl), 256);
+  const size_t o_rd = o;
+  o = align_up(o + sizeof(RoundDesc), 256);
+  const size_t o_pre = o;
+  o = align_up(o + (size_t)NT * (MAX_SLOTS + 1) * 4, 256);
+  const size_t o_ws = o;
+  Layout L = layout_for(g, k, nd, (size_t)n_members, max_edges);
+  if (o_ws + L.total > GST_NOALLOC_SCRATCH_BYTES) return GST_SCRATCH_TOO_SMALL;
+
+  QDev* d_qd = reinterpret_cast<QDev*>(base + o_qd);
+  QCtl* d_ctl = reinterpret_cast<QCtl*>(base + o_ctl);
+  RoundDesc* d_rd = reinterpret_cast<RoundDesc*>(base + o_rd);
+  uint32_t* d_pre = reinterpret_cast<uint32_t*>(base + o_pre);
+  char* ws = base + o_ws;
+
+  QDev q;
+  memset(&q, 0, sizeof(q));
+  q.table = (unsigned long long*)(ws + L.table);
+  q.dist = (uint32_t*)(ws + L.dist);
+  q.dflag = (uint32_t*)(ws + L.dflag);
+  q.sflag = (uint32_t*)(ws + L.sflag);
+  for (int b = 0; b < 4; b++) q.qbuf[b] = (uint32_t*)(ws + L.qbuf) + (size_t)b * L.cap;
+  q.tour = (uint32_t*)(ws + L.tour);
+  q.lbt = (unsigned short*)(ws + L.lbt);
+  q.members = (const uint32_t*)(ws + L.members);
+  q.out_edges = (uint32_t*)(ws + L.edges);
+  q.ctl = d_ctl;
+  q.cap = L.cap;
+  q.nv = g->V;
+  q.n_members = (uint32_t)n_members;
+  q.max_edges = max_edges;
+  q.k = k;
+  q.D = D;
+  q.nd = nd;
+  q.full = (int)((1u << k) - 1u);
+  q.WT = WT;
+  q.phase = PH_SSSP;
+  q.cap_num = std::max(1u, env_u32("GSTB_SSSP_CAP_NUM", 1));
+  q.cap_den = std::max(1u, env_u32("GSTB_SSSP_CAP_DEN", 2));
+  q.in_idx = 0;
+  q.out_idx = 1;
+  q.far_idx = 2;
+  q.far2_idx = 3;
+  q.st = J_INIT;
+  q.act = A_NONE;
+  q.delta_sssp = std::max(1u, env_u32("GSTB_DELTA_SSSP", 16));
+  q.delta_dp = std::max(1u, env_u32("GSTB_DELTA_DP", 4));
+  QCtl c;
+  memset(&c, 0, sizeof(c));
+  c.best = INF32;
+  c.best_full = INF64;
+
+  auto t0 = std::chrono::steady_clock::now();
+  // the array keeps the previous call's contents: reset what must start empty
+  CK(cudaMemsetAsync(q.table, 0xFF, (size_t)g->V * WT * 8, 0));
+  CK(cudaMemsetAsync(q.dist, 0xFF, (size_t)g->V * 8 * 4, 0));
+  CK(cudaMemsetAsync(q.dflag, 0, L.sflag - L.dflag, 0));
+  CK(cudaMemsetAsync(q.sflag, 0, L.qbuf - L.sflag, 0));
+  CK(cudaMemsetAsync(d_rd, 0, sizeof(RoundDesc), 0));
+  // member items v*8 + j, staged through a fixed host buffer
+  {
+    uint32_t stage[1024];
+    size_t n = 0, off = 0;
+    for (int i = 0; i < k; i++) {
+      for (uint64_t t = g->grp_ptr[groups[i]]; t < g->grp_ptr[groups[i] + 1]; t++) {
+        stage[n++] = g->grp_v[t] * 8u + (uint32_t)i;
+        if (n == 1024) {
+          CK(cudaMemcpy((uint32_t*)q.members + off, stage, n * 4, cudaMemcpyHostToDevice));
+          off += n;
+          n = 0;
+        }
+      }
+    }
+    if (n) CK(cudaMemcpy((uint32_t*)q.members + off, stage, n * 4, cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpy(d_qd, &q, sizeof(QDev), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_ctl, &c, sizeof(QCtl), cudaMemcpyHostToDevice));
+
+  GraphDev gd{g->d_beg, g->d_adj, g->V};
+  const unsigned light_grid = (unsigned)g->num_sms * 4, heavy_grid = (unsigned)g->num_sms * 2;
+  const uint32_t R = 6;
+  const uint64_t max_rounds = 1ull << 22;
+  uint64_t rounds = 0;
+  for (;;) {
+    for (uint32_t r = 0; r < R; r++) {
+      k_control<<<1, 1024, 0, 0>>>(d_qd, d_ctl, 1, d_rd, d_pre);
+      k_light<<<light_grid, 256, 0, 0>>>(d_qd, d_rd, d_pre, 1, gd);
+      k_heavy<<<heavy_grid, 256, 0, 0>>>(d_qd, d_rd, d_pre, 1, gd);
+    }
+    CK(cudaGetLastError());
+    g->launches += 3ull * R;
+    rounds += R;
+    CK(cudaMemcpy(&c, d_ctl, sizeof(QCtl), cudaMemcpyDeviceToHost));
+    if (c.done) break;
+    if (rounds > max_rounds) return GST_INTERNAL;
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  gst_status st = (gst_status)c.final_status;
+  if (out) {
+    out->cost = st == GST_OK ? (int32_t)(c.best_full >> 32) : -1;
+    out->root = c.root;
+    out->n_edges = st == GST_OK ? (int32_t)c.n_edges : 0;
+    for (int i = 0; i < GST_NSTATS; i++) out->stats[i] = c.stat[i];
+    out->stats[GST_STAT_TABLE_BYTES] = (uint64_t)g->V * WT * 8;
+    out->device_ms = out->latency_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    if (st == GST_OK) {
+      uint32_t ne = std::min<uint32_t>(c.n_edges, max_edges);
+      int32_t m = out->edges ? std::min<int32_t>((int32_t)ne, out->max_edges) : 0;
+      if (m > 0) CK(cudaMemcpy(out->edges, q.out_edges, (size_t)m * 12, cudaMemcpyDeviceToHost));
+      if ((int64_t)c.n_edges > (int64_t)std::max(out->max_edges, 0) && out->edges) st = GST_TRUNCATED;
+      if (c.n_edges > max_edges) st = GST_TRUNCATED;
+      if (st == GST_OK && m == (int32_t)c.n_edges) {
+        int64_t sum = 0;
+        for (int32_t e = 0; e < m; e++) sum += out->edges[(size_t)e * 3 + 2];
+        if (sum != out->cost) st = GST_INTERNAL;
+      }
+    }
+  }
+  return st;
+}

@@ -24,10 +24,10 @@ LIB_PATH = os.path.join(HERE, "libgstb.so")
 
 GST_OK, GST_NO_SOLUTION, GST_BAD_INPUT, GST_OOM = 0, 1, 2, 3
 GST_DEVICE_TIMEOUT, GST_CUDA_ERROR, GST_QUEUE_OVERFLOW, GST_TRUNCATED = 4, 5, 6, 7
-GST_INTERNAL, GST_BUSY, GST_NOT_FOUND = 8, 9, 10
+GST_INTERNAL, GST_BUSY, GST_NOT_FOUND, GST_SCRATCH_TOO_SMALL = 8, 9, 10, 11
 STATUS_NAMES = {0: "ok", 1: "no solution", 2: "bad input", 3: "out of memory", 4: "device timeout",
                 5: "cuda error", 6: "queue overflow", 7: "truncated", 8: "internal", 9: "busy",
-                10: "not found"}
+                10: "not found", 11: "scratch too small"}
 STAT_NAMES = ["expanded", "sssp_items", "arcs", "updates", "enqueued", "rounds", "merges", "table_bytes"]
 KMAX = 8
 
@@ -62,6 +62,8 @@ def lib():
         L.gst_graph_destroy.restype = None
         L.gst_query.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Result)]
         L.gst_query_batch.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_int]
+        L.gst_query_noalloc.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Result)]
+        L.gst_query_noalloc.restype = ctypes.c_int
         L.gst_status_string.restype = ctypes.c_char_p
         L.gst_graph_num_vertices.restype = u32
         L.gst_graph_num_vertices.argtypes = [vp]
@@ -174,6 +176,19 @@ class Engine:
         st = lib().gst_query(self._h, _ptr(g), len(g), int(D), ctypes.byref(r))
         if st in (GST_CUDA_ERROR, GST_INTERNAL):
             raise GstError(st, "gst_query")
+        return self._unpack(st, r, buf)
+
+    def query_noalloc(self, groups, D: int = -1, max_edges: int = 4096) -> QueryResult:
+        """One query through gst_query_noalloc: every per-query device buffer
+        lives in the library's static scratch array, nothing is allocated."""
+        g = np.ascontiguousarray(groups, dtype=np.uint32)
+        buf = np.zeros(3 * max_edges, dtype=np.uint32)
+        r = _Result()
+        r.max_edges = max_edges
+        r.edges = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+        st = lib().gst_query_noalloc(self._h, _ptr(g), len(g), int(D), ctypes.byref(r))
+        if st in (GST_CUDA_ERROR, GST_INTERNAL):
+            raise GstError(st, "gst_query_noalloc")
         return self._unpack(st, r, buf)
 
     def query_batch(self, queries, Ds=None, max_concurrent: int = 0, max_edges: int = 4096):

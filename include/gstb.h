@@ -51,7 +51,8 @@ typedef enum gst_status {
   GST_TRUNCATED = 7,        /* tree has more edges than the caller's buffer */
   GST_INTERNAL = 8,         /* internal consistency check failed */
   GST_BUSY = 9,             /* serving: no free slot right now (submit again) */
-  GST_NOT_FOUND = 10        /* serving: unknown request id */
+  GST_NOT_FOUND = 10,       /* serving: unknown request id */
+  GST_SCRATCH_TOO_SMALL = 11  /* gst_query_noalloc: workspace exceeds the static scratch */
 } gst_status;
 
 typedef struct gst_graph gst_graph;
@@ -105,6 +106,33 @@ uint64_t gst_graph_num_arcs(const gst_graph* g);
  * tree (the reference's GPU path returns the cost only; its extraction is
  * commented out at DPQ.cu:577-606). */
 gst_status gst_query(gst_graph* g, const uint32_t* groups, int k, int D, gst_result* out);
+
+/* Allocation-free variant of gst_query.  It has no counterpart in the
+ * reference.  Some callers cannot allocate device memory while they answer a
+ * query: a host program that reserves all of the GPU's memory for its own
+ * pool at start-up, so a cudaMalloc from this library would fail or take
+ * memory the host has already promised elsewhere; and a latency-critical
+ * loop in which cudaMalloc / cudaFree, which may synchronise the device,
+ * are not allowed.  This entry point runs the same kernels as gst_query but
+ * keeps every per-query buffer (state table, distances, frontier lists,
+ * control blocks, tree output) in one static device array of
+ * GST_NOALLOC_SCRATCH_BYTES (64 MiB) compiled into this library.  Every GPU
+ * on which the library is loaded holds that array until the process exits.
+ * The call allocates no device or pinned host memory and issues its work on
+ * the legacy default stream; it returns when the GPU work is done.
+ *   - A query whose workspace does not fit returns GST_SCRATCH_TOO_SMALL
+ *     (roughly: V * 2^k * (D+1) states need 8 + 16 + 2^-2 bytes each).
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.
+ *   - All calls share the array; each call re-initialises what must start
+ *     empty.  Calls that overlapped on the GPU would race on it, so the
+ *     library serialises its own calls with a mutex.
+ * Trees are returned with up to 4096 edges (GST_TRUNCATED beyond).  The
+ * call switches to the graph's device for its duration and restores the
+ * caller's current device before returning. */
+#define GST_NOALLOC_SCRATCH_BYTES (64ull << 20)
+gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, int k, int D, gst_result* out);
 
 /* Batched launch: n queries share the device rounds.  groups[i*8 .. i*8+ks[i])
  * lists query i's groups.  results[i].edges/max_edges set by the caller.
