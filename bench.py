@@ -131,21 +131,31 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-# Algorithmic bytes of the round kernel (k_work), from its device counters:
-#   expanded DP state : 64 B  (item id 4, flag 4, state word 8, distance row 32,
-#                              complement word 8, adjacency offsets 8)
-#   distance item     : 56 B  (item id 4, flag 4, distance 4, distance row 32,
-#                              adjacency offsets 8, counters 4)
-#   arc scanned       : 16 B  ({neighbour, weight} 8 + target word 8)
-#   successful update :  8 B, enqueue 8 B (id + flag), merge partner word 8 B
-def algorithmic_bytes(st):
-    return (64 * st["expanded"] + 56 * st["sssp_items"] + 16 * st["arcs"] + 8 * st["updates"]
-            + 8 * st["enqueued"] + 8 * st["merges"])
+# Algorithmic bytes of the two round kernels, from their device counters
+# (the useful bytes each unit of work must move):
+#   k_light, distance item  : 48 B per vertex (item id 4, pending mask 4,
+#                             distance row 32, adjacency offsets 8)
+#            per arc        : 40 B ({neighbour, weight} 8 + target distance row 32)
+#            per update / enqueue : 4 B / 8 B (mask 4 + list entry 4)
+#   k_heavy, DP state       : 66 B (item id 4, flag 4, state word 8, distance
+#                             row 32, complement word 8, bound 2, offsets 8)
+#            per arc        : 18 B ({neighbour, weight} 8, target word 8, bound 2)
+#            per merge partner : 10 B (word 8, bound 2); update 8 B; enqueue 8 B
+#            per bound row  : 32 B read + 2 * 2^k B written (one per vertex)
+def light_bytes(st):
+    return 48 * st["sssp_items"] + 40 * st["sssp_arcs"] + 4 * st["sssp_updates"] + 8 * st["sssp_enqueued"]
+
+
+def heavy_bytes(st, V, ks):
+    lb_rows = sum(V * (32 + 2 * (1 << k)) for k in ks)
+    return (66 * st["expanded"] + 18 * st["arcs"] + 10 * st["merges"] + 8 * st["updates"]
+            + 8 * st["enqueued"] + lb_rows)
 
 
 def traffic_per_byte():
-    """DRAM bytes per algorithmic byte of k_work from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "k_work_traffic.json")
+    """DRAM bytes per algorithmic byte of the dominant round kernel, from the
+    committed ncu summary (profiles/round_kernel_traffic.json), if present."""
+    p = os.path.join(ROOT, "profiles", "round_kernel_traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as f:
@@ -287,6 +297,8 @@ def main():
     ap.add_argument("--batch", type=int, default=90, help="queries per step")
     ap.add_argument("--plain", type=int, default=30, help="queries timed on the plain per-query path")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serve", type=int, default=360, help="queries through the serving loop")
+    ap.add_argument("--inflight", type=int, default=32, help="serving loop concurrency")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -362,17 +374,48 @@ def main():
     value = nq_all / (tot_dev / 1e3)
     e2e_value = nq_all / (tot_wall / 1e3)
 
-    # profiled pass (not timed): k_work device time and counters for the roofline
+    # profiled pass (not timed): round-kernel device time and counters for the roofline
     E.profile(True)
     E.profile_reset()
-    E.query_batch(batch_for(args.warmup))
-    work_ms, work_launches, st = E.profile_read()
+    prof_batch = batch_for(args.warmup)
+    E.query_batch(prof_batch)
+    light_ms, heavy_ms, prof_rounds, st = E.profile_read()
     E.profile(False)
-    alg = algorithmic_bytes(st)
-    achieved = alg / (work_ms / 1e3) / 1e9 if work_ms > 0 else 0.0
+    lb_bytes = light_bytes(st)
+    hb_bytes = heavy_bytes(st, g.V, [len(q) for q in prof_batch])
     peak, peak_kind = measured_peak_hbm()
+    kern = {"k_light": (light_ms, lb_bytes), "k_heavy": (heavy_ms, hb_bytes)}
+    dom = max(kern, key=lambda n: kern[n][0])
+    dom_ms, dom_bytes = kern[dom]
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     tpb = traffic_per_byte()
-    per_launch_alg = alg / max(work_launches, 1)
+    per_launch_alg = dom_bytes / max(prof_rounds, 1)
+
+    # continuous-batching serving loop (closed loop, `--inflight` requests on the device)
+    S = engine.Server(E, max_inflight=args.inflight)
+    n_serve = args.serve
+    serve_q = [pool[(rank * 104729 + 7 * i) % len(pool)] for i in range(n_serve)]
+    lat_serve = []
+    t0 = time.perf_counter()
+    nxt = 0
+    for nxt in range(min(args.inflight, n_serve)):
+        S.submit(nxt, serve_q[nxt])
+    nxt = min(args.inflight, n_serve)
+    done = 0
+    while done < n_serve:
+        got = S.poll()
+        if not got:
+            time.sleep(0.0002)
+            continue
+        for rid, r in got:
+            lat_serve.append(r.latency_ms)
+            done += 1
+            if nxt < n_serve:
+                S.submit(nxt, serve_q[nxt])
+                nxt += 1
+    serve_wall = time.perf_counter() - t0
+    S.close()
+    serve_qps = n_serve / serve_wall
 
     # plain per-query path (one query per call, gst_query), same workload
     plain_lat, plain_dev = [], []
@@ -413,11 +456,15 @@ def main():
             "plain_per_query": {"value": plain_qps, "unit": "queries/s", "queries": len(plain_lat),
                                 "device_ms_p50": pct(plain_dev, 50)},
             "batched_vs_plain": value / plain_qps if plain_qps else None,
-            "roofline": {"bound": "hbm", "kernel": "k_work", "achieved": achieved, "peak": peak,
+            "serve_vs_plain": serve_qps / plain_qps if plain_qps else None,
+            "serve": {"value": serve_qps, "unit": "queries/s", "inflight": args.inflight, "queries": n_serve,
+                      "p50_ms": pct(lat_serve, 50), "p99_ms": pct(lat_serve, 99)},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": (per_launch_alg * tpb) if tpb else None,
-                         "algorithmic_bytes_per_launch": per_launch_alg, "launches": work_launches,
-                         "kernel_ms": work_ms},
+                         "algorithmic_bytes_per_launch": per_launch_alg, "launches": prof_rounds,
+                         "kernel_ms": {"k_light": light_ms, "k_heavy": heavy_ms},
+                         "algorithmic_bytes": {"k_light": lb_bytes, "k_heavy": hb_bytes}},
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": int(launches),

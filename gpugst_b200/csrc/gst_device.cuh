@@ -8,8 +8,10 @@
 //                              cost and parent consistent (no torn parents, unlike the
 //                              reference's separate stores at DPQ.cu:117-121).
 //   dist   u32 [V][8]          shortest distance from query group j to v
-//   dflag  u32 [ceil(V*2^k*nd/16)]  2 bits per state: in-near, in-far
-//   sflag  u32 [ceil(V*8/16)]      2 bits per distance item
+//   dflag  u32 [ceil(V*2^k*nd/8)]   4 bits per state: in-near (two round
+//                                   parities), in-far
+//   sflag  u32 [3][V]              per vertex: groups pending in the near list
+//                                   (two round parities) and in the far list
 //   qbuf   u32 [4][cap]        near-in, near-out, far, far-out work lists of state ids
 //   tour   u32 [k][2^k][k] + [k][2^k] + [8][8]  tour tables P, T2 and group distances
 //   lbt    u16 [V][2^k]        lower bound of completing (v, X) to every group
@@ -60,6 +62,9 @@ enum {
   ST_ENQ = 4,
   ST_ROUNDS = 5,
   ST_MERGES = 6,
+  ST_SSSP_ARCS = 8,
+  ST_SSSP_UPDATES = 9,
+  ST_SSSP_ENQ = 10,
 };
 
 // Written by kernels, read back by the host after every round.
@@ -73,7 +78,7 @@ struct alignas(16) QCtl {
   uint32_t status;   // extraction: 0 ok, 1 no solution, 2 cycle / inconsistency
   uint32_t root;
   unsigned long long best_full;  // min over full states of cost << 32 | payload
-  unsigned long long stat[8];
+  unsigned long long stat[12];
   uint32_t done;     // job finished (set by k_control)
   uint32_t final_status;  // gst_status of the finished job
   uint32_t pad[2];
@@ -108,6 +113,7 @@ struct QDev {
   // state machine
   int32_t st, act;
   uint32_t delta, delta_sssp, delta_dp;
+  uint32_t par;      // parity of the items in (or entering) the near list
 };
 
 struct GraphDev {
@@ -115,6 +121,10 @@ struct GraphDev {
   const uint2* adj;      // [arcs] {neighbour, weight}, each list sorted by (weight, neighbour)
   uint32_t V;
 };
+
+// DP state flags: 4 bits per state, 8 states per word.  Bits 0 and 1 mark
+// "in the near list" for the two round parities, bit 2 "in the far list".
+__device__ __forceinline__ uint32_t dflag_bit(uint32_t s, uint32_t b) { return 1u << (4u * (s & 7u) + b); }
 
 __device__ __forceinline__ unsigned long long pack(uint32_t cost, uint32_t par) {
   return ((unsigned long long)cost << 32) | par;

@@ -64,8 +64,8 @@ struct gst_graph {
   std::mutex mu;
   std::atomic<uint64_t> launches{0};
   bool profile = false;
-  double prof_work_ms = 0;
-  uint64_t prof_work_launches = 0;
+  double prof_light_ms = 0, prof_heavy_ms = 0;
+  uint64_t prof_rounds = 0;
   uint64_t prof_stats[GST_NSTATS] = {0};
 };
 
@@ -122,8 +122,8 @@ Layout layout_for(const gst_graph* g, int k, int nd, size_t n_members, uint32_t 
   size_t o = 0;
   L.table = o; o = align_up(o + states * 8, 256);
   L.dist = o; o = align_up(o + (size_t)g->V * 8 * 4, 256);
-  L.dflag = o; o = align_up(o + ((states + 15) / 16) * 4, 256);
-  L.sflag = o; o = align_up(o + (((size_t)g->V * 8 + 15) / 16) * 4, 256);
+  L.dflag = o; o = align_up(o + ((states + 7) / 8) * 4, 256);
+  L.sflag = o; o = align_up(o + (size_t)g->V * 3 * 4, 256);
   L.qbuf = o; o = align_up(o + 4 * cap * 4, 256);
   L.tour = o; o = align_up(o + ((size_t)k * (1u << k) * k + (size_t)k * (1u << k) + 64) * 4, 256);
   L.lbt = o; o = align_up(o + (size_t)g->V * (1u << k) * 2, 256);
@@ -337,10 +337,11 @@ class Runner {
     const bool prof = g_->profile;
     for (uint32_t r = 0; r < R; r++) {
       k_control<<<1, 1024, 0, stream_>>>(d_qd_, d_ctl_, ns, d_rd_, d_pre_);
-      if (prof) CK(cudaEventRecord(ev_[2 + 2 * r], stream_));
+      if (prof) CK(cudaEventRecord(ev_[2 + 3 * r], stream_));
       k_light<<<light_grid, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
+      if (prof) CK(cudaEventRecord(ev_[3 + 3 * r], stream_));
       k_heavy<<<heavy_grid, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
-      if (prof) CK(cudaEventRecord(ev_[3 + 2 * r], stream_));
+      if (prof) CK(cudaEventRecord(ev_[4 + 3 * r], stream_));
     }
     CK(cudaGetLastError());
     g_->launches += 3ull * R;
@@ -348,10 +349,12 @@ class Runner {
     CK(cudaStreamSynchronize(stream_));
     if (prof) {
       for (uint32_t r = 0; r < R; r++) {
-        float ms = 0;
-        CK(cudaEventElapsedTime(&ms, ev_[2 + 2 * r], ev_[3 + 2 * r]));
-        g_->prof_work_ms += ms;
-        g_->prof_work_launches += 2;
+        float a = 0, b = 0;
+        CK(cudaEventElapsedTime(&a, ev_[2 + 3 * r], ev_[3 + 3 * r]));
+        CK(cudaEventElapsedTime(&b, ev_[3 + 3 * r], ev_[4 + 3 * r]));
+        g_->prof_light_ms += a;
+        g_->prof_heavy_ms += b;
+        g_->prof_rounds++;
       }
     }
     return GST_OK;
@@ -406,7 +409,7 @@ class Runner {
   QDev* h_qd_ = nullptr;
   uint32_t delta_sssp_ = 8, delta_dp_ = 2, max_edges_dev_ = 1u << 16;
   uint32_t cap_num_ = 1, cap_den_ = 2, rounds_per_sync_ = 6;
-  cudaEvent_t ev_[2 + 2 * 64] = {};
+  cudaEvent_t ev_[2 + 3 * 64] = {};
   unsigned light_grid_ = 148 * 4, heavy_grid_ = 148 * 2;
   double last_call_ms_ = 0;
 };
@@ -542,18 +545,21 @@ void gst_profile_enable(gst_graph* g, int on) {
   if (g) g->profile = on != 0;
 }
 
-void gst_profile_read(const gst_graph* g, double* work_ms, uint64_t* work_launches, uint64_t* totals) {
+void gst_profile_read(const gst_graph* g, double* kernel_ms, uint64_t* rounds, uint64_t* totals) {
   if (!g) return;
-  if (work_ms) *work_ms = g->prof_work_ms;
-  if (work_launches) *work_launches = g->prof_work_launches;
+  if (kernel_ms) {
+    kernel_ms[0] = g->prof_light_ms;
+    kernel_ms[1] = g->prof_heavy_ms;
+  }
+  if (rounds) *rounds = g->prof_rounds;
   if (totals)
     for (int t = 0; t < GST_NSTATS; t++) totals[t] = g->prof_stats[t];
 }
 
 void gst_profile_reset(gst_graph* g) {
   if (!g) return;
-  g->prof_work_ms = 0;
-  g->prof_work_launches = 0;
+  g->prof_light_ms = g->prof_heavy_ms = 0;
+  g->prof_rounds = 0;
   for (int t = 0; t < GST_NSTATS; t++) g->prof_stats[t] = 0;
 }
 
@@ -642,6 +648,181 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
     if (g->profile)
       for (int t = 0; t < GST_NSTATS; t++) g->prof_stats[t] += j.ctl.stat[t];
   }
+  return GST_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Serving loop (continuous batching).  A host thread owns a Runner; requests
+// submitted while others run are admitted as soon as a slot and HBM budget
+// free up, and share every device round with the requests already running.
+// ---------------------------------------------------------------------------
+struct gst_server {
+  gst_graph* g = nullptr;
+  Runner* runner = nullptr;
+  std::thread th;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<Job*> pending;
+  std::deque<Job*> finished;
+  bool stop = false;
+  uint64_t budget = 0, in_use = 0;
+  size_t max_inflight = 0, inflight = 0;
+  size_t max_pending = 1u << 20;
+  gst_status fatal = GST_OK;
+};
+
+static void serve_loop(gst_server* S) {
+  cudaSetDevice(S->g->device);
+  for (;;) {
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv.wait(lk, [&] { return S->stop || !S->pending.empty(); });
+      if (S->stop && S->pending.empty()) return;
+    }
+    gst_status st = S->runner->run(
+        [&]() {
+          std::lock_guard<std::mutex> lk(S->mu);
+          while (!S->pending.empty() && S->inflight < S->max_inflight && S->runner->has_free_slot()) {
+            Job* j = S->pending.front();
+            if (S->in_use + j->bytes > S->budget && S->inflight > 0) break;  // wait for memory
+            if (!S->runner->admit(j)) {
+              if (S->inflight == 0) {  // does not fit even alone
+                j->status = GST_OOM;
+                j->done = true;
+                j->t_done = std::chrono::steady_clock::now();
+                S->pending.pop_front();
+                S->finished.push_back(j);
+                continue;
+              }
+              break;
+            }
+            S->pending.pop_front();
+            S->inflight++;
+            S->in_use += j->bytes;
+          }
+        },
+        [&](Job* j) {
+          std::lock_guard<std::mutex> lk(S->mu);
+          S->inflight--;
+          S->in_use -= j->bytes;
+          S->finished.push_back(j);
+        });
+    if (st != GST_OK) {
+      std::lock_guard<std::mutex> lk(S->mu);
+      S->fatal = st;
+      return;
+    }
+  }
+}
+
+extern "C" {
+
+gst_status gst_serve_open(gst_graph* g, uint64_t hbm_budget_bytes, int max_inflight, gst_server** out) {
+  if (!g || !out || g->grp_ptr.empty()) return GST_BAD_INPUT;
+  *out = nullptr;
+  gst_server* S = new gst_server();
+  S->g = g;
+  S->runner = new Runner(g);
+  gst_status st = S->runner->init();
+  if (st != GST_OK) {
+    delete S->runner;
+    delete S;
+    return st;
+  }
+  if (hbm_budget_bytes == 0) {
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    hbm_budget_bytes = (uint64_t)(fr * 0.8);
+  }
+  S->budget = hbm_budget_bytes;
+  S->max_inflight = max_inflight > 0 ? (size_t)max_inflight : (size_t)(MAX_SLOTS - 1);
+  S->th = std::thread(serve_loop, S);
+  *out = S;
+  return GST_OK;
+}
+
+gst_status gst_serve_submit(gst_server* S, uint64_t req_id, const uint32_t* groups, int k, int D) {
+  if (!S || !groups) return GST_BAD_INPUT;
+  Job* j = new Job();
+  j->tag = req_id;
+  j->k = k;
+  j->D = D < 0 ? -1 : D;
+  j->t_submit = std::chrono::steady_clock::now();
+  gst_status ps = (k >= 1 && k <= KMAX) ? GST_OK : GST_BAD_INPUT;
+  if (ps == GST_OK) {
+    memcpy(j->groups, groups, (size_t)k * 4);
+    ps = S->runner->prepare(j);  // host-only validation, no device work
+  }
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (S->fatal != GST_OK) {
+    delete j;
+    return S->fatal;
+  }
+  if (ps != GST_OK) {  // rejected: reported through poll like any result
+    j->status = ps;
+    j->rejected = true;
+    j->done = true;
+    j->t_done = j->t_submit;
+    S->finished.push_back(j);
+    return GST_OK;
+  }
+  if (S->pending.size() >= S->max_pending) {
+    delete j;
+    return GST_BUSY;
+  }
+  S->pending.push_back(j);
+  S->cv.notify_one();
+  return GST_OK;
+}
+
+gst_status gst_serve_poll(gst_server* S, uint64_t* ids, int32_t* statuses, gst_result* results, int max_results,
+                          int* n_out) {
+  if (!S || !n_out || max_results < 0 || (max_results > 0 && (!ids || !statuses))) return GST_BAD_INPUT;
+  std::vector<Job*> got;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    while (!S->finished.empty() && (int)got.size() < max_results) {
+      got.push_back(S->finished.front());
+      S->finished.pop_front();
+    }
+    if (got.empty() && S->fatal != GST_OK) {
+      *n_out = 0;
+      return S->fatal;
+    }
+  }
+  for (size_t i = 0; i < got.size(); i++) {
+    Job* j = got[i];
+    ids[i] = j->tag;
+    if (j->rejected) {
+      statuses[i] = j->status;
+      if (results) {
+        results[i].cost = -1;
+        results[i].n_edges = 0;
+        results[i].latency_ms = 0;
+      }
+    } else {
+      statuses[i] = fill_result(j, results ? &results[i] : nullptr);
+    }
+    delete j;
+  }
+  *n_out = (int)got.size();
+  return GST_OK;
+}
+
+gst_status gst_serve_close(gst_server* S) {
+  if (!S) return GST_BAD_INPUT;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stop = true;
+  }
+  S->cv.notify_all();
+  if (S->th.joinable()) S->th.join();
+  for (Job* j : S->pending) delete j;
+  for (Job* j : S->finished) delete j;
+  delete S->runner;
+  delete S;
   return GST_OK;
 }
 

@@ -39,8 +39,10 @@ __device__ __forceinline__ void enqueue_warp(bool want, uint32_t s, uint32_t cos
   bool nearq = cost < q.theta_hi;
   bool take = false;
   if (want) {
-    uint32_t bit = 1u << (2u * (s & 15u) + (nearq ? 0u : 1u));
-    uint32_t old = atomicOr(&flags[s >> 4], bit);
+    // near entries are flagged with the next round's parity; items of this
+    // round carry the other parity bit, which only their consumer clears
+    uint32_t bit = dflag_bit(s, nearq ? (q.par ^ 1u) : 2u);
+    uint32_t old = atomicOr(&flags[s >> 3], bit);
     take = !(old & bit);
   }
   const unsigned FULL = 0xFFFFFFFFu;
@@ -69,20 +71,13 @@ __device__ __forceinline__ void enqueue_warp(bool want, uint32_t s, uint32_t cos
   if (lane == 0 && cntm) atomicAdd(&q.ctl->stat[ST_ENQ], (unsigned long long)cntm);
 }
 
-// Enqueue for warps whose lanes may serve different queries (distance items
-// are processed by 8-lane groups).  Lanes are aggregated per (query, list)
+// Append for warps whose lanes may serve different queries (distance items
+// are processed by 8-lane groups).  The caller decides `take` (its pending
+// mask went from empty to non-empty); lanes are aggregated per (query, list)
 // with __match_any_sync.  `slot` identifies the query within the launch.
-__device__ __forceinline__ void enqueue_multi(bool want, uint32_t s, uint32_t cost, const QDev& q,
-                                              uint32_t* flags, uint32_t slot, uint32_t lane,
-                                              uint32_t& enq) {
+__device__ __forceinline__ void append_multi(bool take, uint32_t item, bool nearq, const QDev& q,
+                                             uint32_t slot, uint32_t lane, uint32_t& enq) {
   const unsigned FULL = 0xFFFFFFFFu;
-  bool nearq = cost < q.theta_hi;
-  bool take = false;
-  if (want) {
-    uint32_t bit = 1u << (2u * (s & 15u) + (nearq ? 0u : 1u));
-    uint32_t old = atomicOr(&flags[s >> 4], bit);
-    take = !(old & bit);
-  }
   uint32_t key = take ? (slot * 2u + (nearq ? 0u : 1u)) : 0xFFFFFFFFu;
   unsigned m = __match_any_sync(FULL, key);
   uint32_t leader = __ffs(m) - 1;
@@ -96,7 +91,7 @@ __device__ __forceinline__ void enqueue_multi(bool want, uint32_t s, uint32_t co
     uint32_t pos = base + __popc(m & ((1u << lane) - 1u));
     uint32_t* buf = nearq ? q.qbuf[q.out_idx] : q.qbuf[q.far_idx];
     if (pos < q.cap)
-      buf[pos] = s;
+      buf[pos] = item;
     else
       atomicExch(&q.ctl->overflow, 1u);
     enq++;
@@ -130,7 +125,7 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
   const int k = q.k;
   const uint32_t K2 = 1u << k, full = (uint32_t)q.full;
   const uint32_t v = s >> k, p = s & (K2 - 1u);
-  if (lane == 0) atomicAnd(&q.dflag[s >> 4], ~(1u << (2u * (s & 15u))));
+  if (lane == 0) atomicAnd(&q.dflag[s >> 3], ~dflag_bit(s, q.par));
   __syncwarp();
   uint32_t c = __shfl_sync(FULL, (uint32_t)(ld_cg(q.table + s) >> 32), 0);
   uint32_t best = __shfl_sync(FULL, ld_cg(&q.ctl->best), 0);
@@ -189,8 +184,11 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
         if (nc < (uint32_t)(ld_cg(q.table + t) >> 32)) {
           uint32_t lbu = __ldg(lbt + ((size_t)arc.x << k) + comp);
           if ((unsigned long long)nc + lbu <= best) {
-            unsigned long long old = atomicMin(q.table + t, pack(nc, PAR_GROW | v));
-            want = (uint32_t)(old >> 32) > nc;
+            // the pre-check already saw a higher cost: enqueue on it and let the
+            // 64-bit min land without waiting for its result (a concurrent lower
+            // write also enqueues; the flag keeps the list free of duplicates)
+            atomicMin(q.table + t, pack(nc, PAR_GROW | v));
+            want = true;
             upd += want;
           }
         }
@@ -210,20 +208,21 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
       uint32_t t = 0, m32 = 0;
       if (idx < nsub) {
         uint32_t p2 = pdep(idx + 1u, comp);
+        uint32_t qset = p | p2;
         uint32_t c2 = (uint32_t)(ld_cg(row + p2) >> 32);
+        uint32_t cq = (uint32_t)(ld_cg(row + qset) >> 32);
         if (c2 != INF32) {
           merges++;
           unsigned long long m = (unsigned long long)c + c2;
-          uint32_t qset = p | p2;
           // conditional tree merging: 3m <= 2 best (CPUNONHOP.h:941)
-          if (3ull * m <= 2ull * best) {
+          if (3ull * m <= 2ull * best && m < cq) {
             uint32_t lbq = __ldg(lbt + ((size_t)v << k) + (full ^ qset));
             if (m + lbq <= best) {
               m32 = (uint32_t)m;
               t = (v << k) | qset;
-              unsigned long long old = atomicMin(q.table + t, pack(m32, PAR_MERGE | p));
-              want = (uint32_t)(old >> 32) > m32;
-              upd += want;
+              atomicMin(q.table + t, pack(m32, PAR_MERGE | p));
+              want = true;
+              upd++;
             }
           }
         }
@@ -254,7 +253,7 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
   const uint32_t K2 = 1u << k, full = (uint32_t)q.full;
   const uint32_t d = s % (uint32_t)nd, vp = s / (uint32_t)nd;
   const uint32_t v = vp >> k, p = vp & (K2 - 1u);
-  if (lane == 0) atomicAnd(&q.dflag[s >> 4], ~(1u << (2u * (s & 15u))));
+  if (lane == 0) atomicAnd(&q.dflag[s >> 3], ~dflag_bit(s, q.par));
   __syncwarp();
   uint32_t c = __shfl_sync(FULL, (uint32_t)(ld_cg(q.table + s) >> 32), 0);
   uint32_t best = __shfl_sync(FULL, ld_cg(&q.ctl->best), 0);
@@ -292,8 +291,11 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
         if (nc < (uint32_t)(ld_cg(q.table + t) >> 32)) {
           uint32_t lbu = __ldg(lbt + ((size_t)arc.x << k) + comp);
           if ((unsigned long long)nc + lbu <= best) {
-            unsigned long long old = atomicMin(q.table + t, pack(nc, PAR_GROW | v));
-            want = (uint32_t)(old >> 32) > nc;
+            // the pre-check already saw a higher cost: enqueue on it and let the
+            // 64-bit min land without waiting for its result (a concurrent lower
+            // write also enqueues; the flag keeps the list free of duplicates)
+            atomicMin(q.table + t, pack(nc, PAR_GROW | v));
+            want = true;
             upd += want;
           }
         }
@@ -333,10 +335,10 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
               atomicMin(&q.ctl->best_full, ((unsigned long long)m32 << 32) | (v * 8u + ndd));
             } else {
               uint32_t lbq = __ldg(lbt + ((size_t)v << k) + (full ^ qset));
-              if (m + lbq <= best) {
-                unsigned long long old = atomicMin(q.table + t, pack(m32, par));
-                want = (uint32_t)(old >> 32) > m32;
-                upd += want;
+              if (m + lbq <= best && m32 < (uint32_t)(ld_cg(q.table + t) >> 32)) {
+                atomicMin(q.table + t, pack(m32, par));
+                want = true;
+                upd++;
               }
             }
           }
@@ -372,6 +374,19 @@ __device__ __forceinline__ uint32_t find_slot(const uint32_t* __restrict__ pre, 
   return (uint32_t)lo;
 }
 
+// Same search over a prefix array staged in shared memory.
+__device__ __forceinline__ uint32_t find_slot_s(const uint32_t* pre, int nslots, uint32_t it) {
+  int lo = 0, hi = nslots;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (pre[mid] <= it)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return (uint32_t)lo;
+}
+
 // ---------------------------------------------------------------------------
 // Distance items: one warp task = 4 items, 8 lanes each.  The weight-sorted
 // adjacency usually leaves only a few arcs under the limit, so a full warp
@@ -394,9 +409,9 @@ __device__ __forceinline__ void sssp_flush(SsspCounters& sc, uint32_t sl) {
   }
   if (sc.cur && sl == 0) {
     if (sc.items) atomicAdd(&sc.cur->stat[ST_SSSP], (unsigned long long)sc.items);
-    if (a) atomicAdd(&sc.cur->stat[ST_ARCS], (unsigned long long)a);
-    if (u) atomicAdd(&sc.cur->stat[ST_UPDATES], (unsigned long long)u);
-    if (e) atomicAdd(&sc.cur->stat[ST_ENQ], (unsigned long long)e);
+    if (a) atomicAdd(&sc.cur->stat[ST_SSSP_ARCS], (unsigned long long)a);
+    if (u) atomicAdd(&sc.cur->stat[ST_SSSP_UPDATES], (unsigned long long)u);
+    if (e) atomicAdd(&sc.cur->stat[ST_SSSP_ENQ], (unsigned long long)e);
   }
   sc.items = sc.arcs = sc.upd = sc.enq = 0;
 }
@@ -407,12 +422,11 @@ __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restric
   const uint32_t sub = lane >> 3, sl = lane & 7u, gbase = lane & ~7u;
   const uint32_t it = task * 4u + sub;
   const bool valid = it < total;
-  const uint32_t slot = valid ? find_slot(pre, nslots, it) : 0u;
+  const uint32_t slot = valid ? find_slot_s(pre, nslots, it) : 0u;
   const QDev& q = qd[slot];
   // flush the group's counters when it changes query (group-uniform decision)
   bool change = valid && q.ctl != sc.cur;
   if (__any_sync(FULL, change)) {
-    // lanes of groups that change flush; others keep accumulating
     unsigned cm = __ballot_sync(FULL, change);
     bool mine = (cm >> gbase) & 1u;
     uint32_t a = sc.arcs, u = sc.upd, e = sc.enq;
@@ -425,41 +439,55 @@ __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restric
     if (mine) {
       if (sc.cur && sl == 0) {
         if (sc.items) atomicAdd(&sc.cur->stat[ST_SSSP], (unsigned long long)sc.items);
-        if (a) atomicAdd(&sc.cur->stat[ST_ARCS], (unsigned long long)a);
-        if (u) atomicAdd(&sc.cur->stat[ST_UPDATES], (unsigned long long)u);
-        if (e) atomicAdd(&sc.cur->stat[ST_ENQ], (unsigned long long)e);
+        if (a) atomicAdd(&sc.cur->stat[ST_SSSP_ARCS], (unsigned long long)a);
+        if (u) atomicAdd(&sc.cur->stat[ST_SSSP_UPDATES], (unsigned long long)u);
+        if (e) atomicAdd(&sc.cur->stat[ST_SSSP_ENQ], (unsigned long long)e);
       }
       sc.items = sc.arcs = sc.upd = sc.enq = 0;
       sc.cur = q.ctl;
     }
   }
-  const uint32_t s = valid ? q.qbuf[q.in_idx][it - __ldcg(pre + slot)] : 0u;
-  const uint32_t v = s >> 3, jg = s & 7u;
-  if (valid && sl == 0) atomicAnd(&q.sflag[s >> 4], ~(1u << (2u * (s & 15u))));
-  __syncwarp();
-  uint32_t d = __shfl_sync(FULL, valid ? ld_cg(q.dist + s) : INF32, gbase);
+  const uint32_t V = q.nv;
+  const uint32_t v = valid ? q.qbuf[q.in_idx][it - pre[slot]] : 0u;
+  // take the groups whose distance at v changed into this window
+  uint32_t m = 0;
+  if (valid && sl == 0) m = atomicExch(&q.sflag[(size_t)q.par * V + v], 0u);
+  m = __shfl_sync(FULL, m, gbase);
+  const int k = valid ? q.k : 0;
+  // lane sl holds d_sl(v)
+  const uint32_t dj = (valid && sl < (uint32_t)k) ? ld_cg(q.dist + (size_t)v * 8 + sl) : INF32;
   uint32_t best = __shfl_sync(FULL, valid ? ld_cg(&q.ctl->best) : 0u, gbase);
-  bool active = valid && d != INF32 && d <= best;
   // star bound at v (unbounded queries only): v joined to every group by
   // shortest paths, a feasible tree (one-label completion, CPUNONHOP.h:684-699)
   {
-    bool lanev = active && q.D < 0 && sl < (uint32_t)q.k;
-    uint32_t dj = lanev ? ld_cg(q.dist + (size_t)v * 8 + sl) : 0u;
+    bool lanev = valid && q.D < 0 && sl < (uint32_t)k;
     unsigned bad = __ballot_sync(FULL, lanev && dj == INF32);
-    unsigned long long sum = dj;
+    unsigned long long sum = lanev ? dj : 0u;
     sum += __shfl_xor_sync(FULL, sum, 4);
     sum += __shfl_xor_sync(FULL, sum, 2);
     sum += __shfl_xor_sync(FULL, sum, 1);
-    if (active && q.D < 0 && sl == 0 && ((bad >> gbase) & 0xFFu) == 0 && sum < best)
+    if (valid && q.D < 0 && sl == 0 && ((bad >> gbase) & 0xFFu) == 0 && sum < best)
       atomicMin(&q.ctl->best, (uint32_t)sum);
   }
   best = __shfl_sync(FULL, valid ? ld_cg(&q.ctl->best) : 0u, gbase);
   // distances beyond cap(best) cannot lower a bound below best: skip them
   const uint32_t capb = valid ? (uint32_t)((unsigned long long)best * q.cap_num / q.cap_den) : 0u;
-  active = active && d <= capb;
-  const uint32_t lim = active ? capb - d : 0u;
+  const bool rl = valid && sl < (uint32_t)k && ((m >> sl) & 1u) && dj <= capb;
+  const uint32_t rm = (__ballot_sync(FULL, rl) >> gbase) & 0xFFu;  // groups to relax
+  uint32_t dmin = rl ? dj : INF32;
+  dmin = min(dmin, __shfl_xor_sync(FULL, dmin, 4));
+  dmin = min(dmin, __shfl_xor_sync(FULL, dmin, 2));
+  dmin = min(dmin, __shfl_xor_sync(FULL, dmin, 1));
+  uint32_t d[KMAX];
+#pragma unroll
+  for (int t = 0; t < KMAX; t++) d[t] = __shfl_sync(FULL, dj, gbase + t);
+  const bool active = rm != 0;
+  const uint32_t lim = active ? capb - dmin : 0u;
   const uint32_t a0 = active ? __ldg(g.beg + v) : 0u, a1 = active ? __ldg(g.beg + v + 1) : 0u;
   if (active && sl == 0) sc.items++;
+  const uint32_t thi = valid ? q.theta_hi : 0u;
+  uint32_t* pnext = valid ? q.sflag + (size_t)(q.par ^ 1u) * V : nullptr;
+  uint32_t* pfar = valid ? q.sflag + (size_t)2 * V : nullptr;
   bool done = !active;
   for (uint32_t off = 0;; off += 8) {
     bool more = !done && a0 + off < a1;
@@ -468,19 +496,33 @@ __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restric
     bool in = more && a < a1;
     uint2 arc = in ? __ldg(g.adj + a) : make_uint2(0, 0xFFFFFFFFu);
     bool over = in && arc.y > lim;
-    bool want = false;
-    uint32_t t = 0, nd = 0;
+    bool takeN = false, takeF = false;
     if (in && !over) {
       sc.arcs++;
-      nd = d + arc.y;
-      t = arc.x * 8u + jg;
-      if (nd < ld_cg(q.dist + t)) {
-        uint32_t old = atomicMin(q.dist + t, nd);
-        want = nd < old;
-        sc.upd += want;
+      const uint32_t u = arc.x;
+      const uint4* row = reinterpret_cast<const uint4*>(q.dist + (size_t)u * 8);
+      uint4 ra = __ldcg(row), rb = __ldcg(row + 1);
+      uint32_t du[8] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
+      uint32_t nn = 0, nf = 0;
+#pragma unroll
+      for (int t = 0; t < KMAX; t++) {
+        if ((rm >> t) & 1u) {
+          uint32_t nd = d[t] + arc.y;
+          if (nd <= capb && nd < du[t]) {
+            atomicMin(q.dist + (size_t)u * 8 + t, nd);  // result not needed
+            if (nd < thi)
+              nn |= 1u << t;
+            else
+              nf |= 1u << t;
+            sc.upd++;
+          }
+        }
       }
+      if (nn) takeN = atomicOr(pnext + u, nn) == 0u;
+      if (nf) takeF = atomicOr(pfar + u, nf) == 0u;
     }
-    enqueue_multi(want, t, nd, q, q.sflag, slot, lane, sc.enq);
+    append_multi(takeN, arc.x, true, q, slot, lane, sc.enq);
+    append_multi(takeF, arc.x, false, q, slot, lane, sc.enq);
     unsigned stop = __ballot_sync(FULL, over || (more && a + 1 >= a1));
     if ((stop >> gbase) & 0xFFu) done = true;  // sorted by weight: the rest is heavier
   }
@@ -489,43 +531,54 @@ __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restric
 // Near-far split of one far item: cost in [theta_lo, theta_hi) -> near list;
 // above -> far-out list; below theta_lo it was already expanded at that cost
 // (every new cost is >= the cost of the item that produced it) -> dropped.
+// Distance items are vertices with a mask of pending groups; DP items are
+// states.  Items moved to the near list carry the parity of the next round.
+__device__ __forceinline__ void push_list(const QDev& q, uint32_t* cnt, uint32_t* buf, uint32_t item) {
+  uint32_t pos = atomicAdd(cnt, 1u);
+  if (pos < q.cap)
+    buf[pos] = item;
+  else
+    atomicExch(&q.ctl->overflow, 1u);
+}
+
 __device__ void split_item(const QDev& q, uint32_t s) {
-  uint32_t* flags = q.phase == PH_SSSP ? q.sflag : q.dflag;
-  uint32_t cost = q.phase == PH_SSSP ? ld_cg(q.dist + s) : (uint32_t)(ld_cg(q.table + s) >> 32);
   uint32_t best = ld_cg(&q.ctl->best);
-  uint32_t sh = 2u * (s & 15u);
-  if (cost < q.theta_lo || cost == INF32 || cost > best) {
-    atomicAnd(&flags[s >> 4], ~(2u << sh));
-  } else if (cost < q.theta_hi) {
-    atomicAnd(&flags[s >> 4], ~(2u << sh));
-    uint32_t old = atomicOr(&flags[s >> 4], 1u << sh);
-    if (!(old & (1u << sh))) {
-      uint32_t pos = atomicAdd(&q.ctl->n_near, 1u);
-      if (pos < q.cap)
-        q.qbuf[q.out_idx][pos] = s;
+  if (q.phase == PH_SSSP) {
+    const uint32_t V = q.nv;
+    const uint32_t capb = (uint32_t)((unsigned long long)best * q.cap_num / q.cap_den);
+    uint32_t fm = atomicExch(&q.sflag[(size_t)2 * V + s], 0u);
+    uint32_t nb = 0, kb = 0;
+    for (int t = 0; t < q.k; t++) {
+      if (!((fm >> t) & 1u)) continue;
+      uint32_t d = ld_cg(q.dist + (size_t)s * 8 + t);
+      if (d < q.theta_lo || d == INF32 || d > capb) continue;
+      if (d < q.theta_hi)
+        nb |= 1u << t;
       else
-        atomicExch(&q.ctl->overflow, 1u);
+        kb |= 1u << t;
     }
+    if (nb && atomicOr(&q.sflag[(size_t)q.par * V + s], nb) == 0u) push_list(q, &q.ctl->n_near, q.qbuf[q.out_idx], s);
+    if (kb && atomicOr(&q.sflag[(size_t)2 * V + s], kb) == 0u) push_list(q, &q.ctl->n_far2, q.qbuf[q.far2_idx], s);
+    return;
+  }
+  uint32_t cost = (uint32_t)(ld_cg(q.table + s) >> 32);
+  if (cost < q.theta_lo || cost == INF32 || cost > best) {
+    atomicAnd(&q.dflag[s >> 3], ~dflag_bit(s, 2u));
+  } else if (cost < q.theta_hi) {
+    atomicAnd(&q.dflag[s >> 3], ~dflag_bit(s, 2u));
+    uint32_t bit = dflag_bit(s, q.par);
+    uint32_t old = atomicOr(&q.dflag[s >> 3], bit);
+    if (!(old & bit)) push_list(q, &q.ctl->n_near, q.qbuf[q.out_idx], s);
   } else {
-    uint32_t pos = atomicAdd(&q.ctl->n_far2, 1u);
-    if (pos < q.cap)
-      q.qbuf[q.far2_idx][pos] = s;
-    else
-      atomicExch(&q.ctl->overflow, 1u);
+    push_list(q, &q.ctl->n_far2, q.qbuf[q.far2_idx], s);
   }
 }
 
-// Member item v*8+j -> distance 0, first near list.
-__device__ void sseed_item(const QDev& q, uint32_t s) {
-  q.dist[s] = 0;
-  uint32_t old = atomicOr(&q.sflag[s >> 4], 1u << (2u * (s & 15u)));
-  if (!(old & (1u << (2u * (s & 15u))))) {
-    uint32_t pos = atomicAdd(&q.ctl->n_near, 1u);
-    if (pos < q.cap)
-      q.qbuf[q.out_idx][pos] = s;
-    else
-      atomicExch(&q.ctl->overflow, 1u);
-  }
+// Member item v*8+j -> distance 0; the vertex enters the first near list.
+__device__ void sseed_item(const QDev& q, uint32_t item) {
+  uint32_t v = item >> 3, j = item & 7u;
+  q.dist[item] = 0;
+  if (atomicOr(&q.sflag[(size_t)q.par * q.nv + v], 1u << j) == 0u) push_list(q, &q.ctl->n_near, q.qbuf[q.out_idx], v);
 }
 
 // Cost-0 states: every non-empty subset of a member's mask (DPQ.cu:341-358).
@@ -544,14 +597,8 @@ __device__ void dseed_item(const QDev& q, uint32_t item) {
       atomicMin(&q.ctl->best_full, q.phase == PH_HOP ? (unsigned long long)(v * 8u) : (unsigned long long)v);
       continue;
     }
-    uint32_t old = atomicOr(&q.dflag[s >> 4], 1u << (2u * (s & 15u)));
-    if (!(old & (1u << (2u * (s & 15u))))) {
-      uint32_t pos = atomicAdd(&q.ctl->n_near, 1u);
-      if (pos < q.cap)
-        q.qbuf[q.out_idx][pos] = s;
-      else
-        atomicExch(&q.ctl->overflow, 1u);
-    }
+    uint32_t bit = dflag_bit(s, q.par);
+    if (!(atomicOr(&q.dflag[s >> 3], bit) & bit)) push_list(q, &q.ctl->n_near, q.qbuf[q.out_idx], s);
   }
 }
 
@@ -734,6 +781,7 @@ __device__ __forceinline__ void absorb(QDev& q, QCtl& c) {
       t = q.in_idx; q.in_idx = q.out_idx; q.out_idx = t;
       q.n_in = c.n_near;
       q.n_far = c.n_far;
+      q.par ^= 1u;  // producers of the round flagged the next items with the other parity
       break;
     case A_SPLIT:
       t = q.in_idx; q.in_idx = q.out_idx; q.out_idx = t;
@@ -929,6 +977,10 @@ __global__ void __launch_bounds__(256) k_light(const QDev* __restrict__ qd, cons
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t ntasks = __ldcg(&rd->light_tasks);
+  // the distance items' prefix over slots, staged once per block
+  __shared__ uint32_t s_pre[MAX_SLOTS + 1];
+  for (int i = threadIdx.x; i <= nslots; i += blockDim.x) s_pre[i] = __ldcg(pre + T_SSSP * (MAX_SLOTS + 1) + i);
+  __syncthreads();
   SsspCounters sc;
   for (uint32_t task = warp; task < ntasks; task += nwarps) {
     int t = 0;
@@ -937,7 +989,7 @@ __global__ void __launch_bounds__(256) k_light(const QDev* __restrict__ qd, cons
     const uint32_t* P = pre + t * (MAX_SLOTS + 1);
     const uint32_t total = __ldcg(&rd->items[t]);
     if (t == T_SSSP) {
-      sssp_task(qd, P, nslots, total, local, g, lane, sc);
+      sssp_task(qd, s_pre, nslots, total, local, g, lane, sc);
     } else if (t == T_TOUR) {
       tour_warp(qd[find_slot(P, nslots, local)], lane);
     } else if (t == T_EXTRACT) {
@@ -969,6 +1021,12 @@ __global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, cons
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t ntasks = __ldcg(&rd->heavy_tasks);
   const uint32_t dp0 = __ldcg(&rd->task_off[T_DP]), hop0 = __ldcg(&rd->task_off[T_HOP]);
+  __shared__ uint32_t s_dp[MAX_SLOTS + 1], s_hop[MAX_SLOTS + 1];
+  for (int i = threadIdx.x; i <= nslots; i += blockDim.x) {
+    s_dp[i] = __ldcg(pre + T_DP * (MAX_SLOTS + 1) + i);
+    s_hop[i] = __ldcg(pre + T_HOP * (MAX_SLOTS + 1) + i);
+  }
+  __syncthreads();
   for (uint32_t task = warp; task < ntasks; task += nwarps) {
     if (task < dp0) {  // lower-bound table rows, one vertex per lane
       const uint32_t* P = pre + T_LB * (MAX_SLOTS + 1);
@@ -981,10 +1039,10 @@ __global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, cons
     }
     const bool hop = task >= hop0;
     const uint32_t it = hop ? task - hop0 : task - dp0;
-    const uint32_t* P = pre + (hop ? T_HOP : T_DP) * (MAX_SLOTS + 1);
-    const uint32_t slot = find_slot(P, nslots, it);
+    const uint32_t* P = hop ? s_hop : s_dp;
+    const uint32_t slot = find_slot_s(P, nslots, it);
     const QDev& q = qd[slot];
-    const uint32_t s = q.qbuf[q.in_idx][it - __ldcg(P + slot)];
+    const uint32_t s = q.qbuf[q.in_idx][it - P[slot]];
     if (hop)
       hop_item(q, g, s, lane);
     else

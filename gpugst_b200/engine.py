@@ -28,7 +28,9 @@ GST_INTERNAL, GST_BUSY, GST_NOT_FOUND, GST_SCRATCH_TOO_SMALL = 8, 9, 10, 11
 STATUS_NAMES = {0: "ok", 1: "no solution", 2: "bad input", 3: "out of memory", 4: "device timeout",
                 5: "cuda error", 6: "queue overflow", 7: "truncated", 8: "internal", 9: "busy",
                 10: "not found", 11: "scratch too small"}
-STAT_NAMES = ["expanded", "sssp_items", "arcs", "updates", "enqueued", "rounds", "merges", "table_bytes"]
+STAT_NAMES = ["expanded", "sssp_items", "arcs", "updates", "enqueued", "rounds", "merges", "table_bytes",
+              "sssp_arcs", "sssp_updates", "sssp_enqueued", "reserved"]
+NSTATS = len(STAT_NAMES)
 KMAX = 8
 
 
@@ -41,7 +43,7 @@ class GstError(RuntimeError):
 class _Result(ctypes.Structure):
     _fields_ = [("cost", ctypes.c_int32), ("root", ctypes.c_uint32), ("n_edges", ctypes.c_int32),
                 ("max_edges", ctypes.c_int32), ("edges", ctypes.POINTER(ctypes.c_uint32)),
-                ("stats", ctypes.c_uint64 * 8), ("device_ms", ctypes.c_double),
+                ("stats", ctypes.c_uint64 * 12), ("device_ms", ctypes.c_double),
                 ("latency_ms", ctypes.c_double)]
 
 
@@ -73,10 +75,16 @@ def lib():
         L.gst_kernel_launches.restype = u64
         L.gst_profile_enable.argtypes = [vp, ctypes.c_int]
         L.gst_profile_enable.restype = None
-        L.gst_profile_read.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(u64), vp]
+        L.gst_profile_read.argtypes = [vp, vp, ctypes.POINTER(u64), vp]
         L.gst_profile_read.restype = None
         L.gst_profile_reset.argtypes = [vp]
         L.gst_profile_reset.restype = None
+        L.gst_serve_open.argtypes = [vp, u64, ctypes.c_int, ctypes.POINTER(vp)]
+        L.gst_serve_submit.argtypes = [vp, u64, vp, ctypes.c_int, ctypes.c_int]
+        L.gst_serve_poll.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.gst_serve_close.argtypes = [vp]
+        for name in ("gst_serve_open", "gst_serve_submit", "gst_serve_poll", "gst_serve_close"):
+            getattr(L, name).restype = ctypes.c_int
         for name in ("gst_graph_create", "gst_groups_set", "gst_query", "gst_query_batch"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
@@ -160,11 +168,12 @@ class Engine:
         lib().gst_profile_reset(self._h)
 
     def profile_read(self):
-        ms = ctypes.c_double(0)
+        """(light_ms, heavy_ms, rounds, summed stats) accumulated while profiling."""
+        ms = np.zeros(2, dtype=np.float64)
         n = ctypes.c_uint64(0)
-        tot = np.zeros(8, dtype=np.uint64)
-        lib().gst_profile_read(self._h, ctypes.byref(ms), ctypes.byref(n), _ptr(tot))
-        return ms.value, n.value, {name: int(tot[i]) for i, name in enumerate(STAT_NAMES)}
+        tot = np.zeros(NSTATS, dtype=np.uint64)
+        lib().gst_profile_read(self._h, _ptr(ms), ctypes.byref(n), _ptr(tot))
+        return float(ms[0]), float(ms[1]), n.value, {name: int(tot[i]) for i, name in enumerate(STAT_NAMES)}
 
     def query(self, groups, D: int = -1, max_edges: int = 4096) -> QueryResult:
         """One synchronous query (gst_query)."""
@@ -217,3 +226,53 @@ class Engine:
             if r.status in (GST_CUDA_ERROR, GST_INTERNAL):
                 raise GstError(r.status, "gst_query_batch")
         return out
+
+
+class Server:
+    """Continuous-batching serving loop over an Engine's graph (gst_serve_*)."""
+
+    def __init__(self, eng: Engine, hbm_budget: int = 0, max_inflight: int = 0):
+        self._eng = eng
+        h = ctypes.c_void_p()
+        st = lib().gst_serve_open(eng._h, int(hbm_budget), int(max_inflight), ctypes.byref(h))
+        if st != GST_OK:
+            raise GstError(st, "gst_serve_open")
+        self._h = h
+
+    def submit(self, req_id: int, groups, D: int = -1) -> int:
+        g = np.ascontiguousarray(groups, dtype=np.uint32)
+        return int(lib().gst_serve_submit(self._h, int(req_id), _ptr(g), len(g), int(D)))
+
+    def poll(self, max_results: int = 1024, max_edges: int = 0):
+        """Finished requests as a list of (req_id, QueryResult)."""
+        ids = np.zeros(max_results, dtype=np.uint64)
+        sts = np.zeros(max_results, dtype=np.int32)
+        res = (_Result * max_results)()
+        bufs = []
+        for i in range(max_results):
+            if max_edges:
+                b = np.zeros(3 * max_edges, dtype=np.uint32)
+                bufs.append(b)
+                res[i].edges = b.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+            res[i].max_edges = max_edges
+        n = ctypes.c_int(0)
+        st = lib().gst_serve_poll(self._h, _ptr(ids), _ptr(sts), ctypes.cast(res, ctypes.c_void_p), max_results,
+                                  ctypes.byref(n))
+        if st != GST_OK:
+            raise GstError(st, "gst_serve_poll")
+        out = []
+        for i in range(n.value):
+            buf = bufs[i] if max_edges else np.zeros(0, dtype=np.uint32)
+            out.append((int(ids[i]), Engine._unpack(int(sts[i]), res[i], buf)))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gst_serve_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -62,13 +62,17 @@ typedef struct gst_graph gst_graph;
 enum {
   GST_STAT_EXPANDED = 0,    /* DP states expanded (reference process_num, DPQ.cu:514) */
   GST_STAT_SSSP_ITEMS = 1,  /* distance items expanded */
-  GST_STAT_ARCS = 2,        /* arcs scanned (grow + distance) */
-  GST_STAT_UPDATES = 3,     /* successful atomic lowerings */
-  GST_STAT_ENQUEUED = 4,    /* frontier insertions */
+  GST_STAT_ARCS = 2,        /* arcs scanned by DP grows */
+  GST_STAT_UPDATES = 3,     /* successful DP state lowerings */
+  GST_STAT_ENQUEUED = 4,    /* DP frontier insertions */
   GST_STAT_ROUNDS = 5,      /* device rounds */
   GST_STAT_MERGES = 6,      /* merge candidates evaluated */
   GST_STAT_TABLE_BYTES = 7, /* bytes of the state table */
-  GST_NSTATS = 8
+  GST_STAT_SSSP_ARCS = 8,   /* arcs scanned by distance items */
+  GST_STAT_SSSP_UPDATES = 9,  /* successful distance lowerings */
+  GST_STAT_SSSP_ENQUEUED = 10, /* distance frontier insertions */
+  GST_STAT_RESERVED = 11,
+  GST_NSTATS = 12
 };
 
 typedef struct gst_result {
@@ -149,6 +153,10 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
  * (the reference runs queries serially, exp_GPU_nonHop.h:97-138). */
 typedef struct gst_server gst_server;
 
+/* hbm_budget_bytes: device bytes the admitted queries' workspaces may hold
+ * at once (0 = 80% of the free memory at open); max_inflight: queries on the
+ * device at once (0 = up to 1023).  Each result's latency_ms is the time from
+ * submission to completion. */
 gst_status gst_serve_open(gst_graph* g, uint64_t hbm_budget_bytes, int max_inflight,
                           gst_server** out);
 /* Never blocks.  Copies the groups.  GST_BUSY if the pending queue is full. */
@@ -158,18 +166,21 @@ gst_status gst_serve_submit(gst_server* s, uint64_t req_id, const uint32_t* grou
  * caller; pass max_edges 0 to skip trees).  ids[i] and statuses[i] filled. */
 gst_status gst_serve_poll(gst_server* s, uint64_t* ids, int32_t* statuses, gst_result* results,
                           int max_results, int* n_out);
-/* Host timestamps of a finished request, valid after poll: submit -> done (ms). */
+/* Stops the loop after the submitted requests finish and frees everything;
+ * results not polled by then are discarded. */
 gst_status gst_serve_close(gst_server* s);
 
 const char* gst_status_string(gst_status st);
 
 /* Diagnostics (no reference counterpart).  Kernel launches issued by this
- * graph's engine so far, and, when profiling is on, the accumulated device
- * time and launch count of the round kernel (k_work) plus the summed
- * GST_STAT_* counters of the finished queries. */
+ * graph's engine so far, and, when profiling is on (gst_query_batch calls
+ * only), the accumulated device time of the two round kernels
+ * (kernel_ms[0] = k_light: distance items, splits, seeds, tours,
+ * extraction; kernel_ms[1] = k_heavy: lower-bound rows and DP states), the
+ * number of rounds, and the summed GST_STAT_* counters of finished queries. */
 uint64_t gst_kernel_launches(const gst_graph* g);
 void gst_profile_enable(gst_graph* g, int on);
-void gst_profile_read(const gst_graph* g, double* work_ms, uint64_t* work_launches,
+void gst_profile_read(const gst_graph* g, double kernel_ms[2], uint64_t* rounds,
                       uint64_t stats_totals[GST_NSTATS]);
 void gst_profile_reset(gst_graph* g);
 

@@ -163,3 +163,37 @@ def test_edge_cases(gst_lib, oracle_mod):
         if r is not None:
             assert r.status == eng.GST_BAD_INPUT, (bad_q, bad_d, r.status)
     E.close()
+
+
+def test_serve_alone_vs_in_the_mix(gst_lib, c1):
+    """Continuous batching: requests submitted while others run give the same
+    cost as the same request run alone (integer costs: equal)."""
+    import time
+    eng = gst_lib
+    g, gr, qs = c1
+    rng = np.random.default_rng(9)
+    reqs = []
+    for i in range(60):
+        k = int(rng.integers(2, 6))
+        reqs.append((rng.choice(gr.n_groups, size=k, replace=False).astype(np.uint32), int(rng.choice([-1, 2, 3, 4]))))
+    E = _engine(eng, g, gr)
+    alone = [E.query(q, D=D) for q, D in reqs]
+    S = eng.Server(E, max_inflight=16)
+    got = {}
+    for i, (q, D) in enumerate(reqs):
+        assert S.submit(i, q, D) == eng.GST_OK
+        if i % 7 == 0:
+            for rid, r in S.poll():
+                got[rid] = r
+    t0 = time.time()
+    while len(got) < len(reqs) and time.time() - t0 < 120:
+        for rid, r in S.poll(max_edges=4096):
+            got[rid] = r
+        time.sleep(0.002)
+    S.close()
+    E.close()
+    assert len(got) == len(reqs)
+    for i, a in enumerate(alone):
+        assert got[i].status == a.status, (i, got[i].status, a.status)
+        assert got[i].cost == a.cost, (i, got[i].cost, a.cost)
+        assert got[i].latency_ms >= 0
