@@ -43,8 +43,19 @@ struct RoundDesc {
   uint32_t task_off[NT + 1];  // warp-task offsets (light types, then heavy types restart at 0)
   uint32_t light_tasks, heavy_tasks;
   uint32_t n_live;        // slots whose job is not finished
-  uint32_t pad;
+  uint32_t n_big;         // hub arc chunks queued by k_light for k_heavy this round
+  // hub arc chunks: {slot | groups << 16, vertex, first arc, end arc}; set
+  // once by the host (null / 0 disables chunking)
+  uint4* big;
+  uint32_t big_cap;
+  uint32_t hub_min_deg;   // only items with at least this many arcs under their limit are chunked
+  uint32_t hub_min_rest;  // ... and only when at least this many arcs remain under the limit
+  uint32_t hub_max_items; // chunk only in rounds with fewer distance items (latency-bound rounds)
+  uint32_t hub_on;        // set by k_control for the current round
+  uint32_t pad3;
 };
+constexpr uint32_t HUB_CHUNK = 256;     // arcs per chunk (one warp)
+constexpr uint32_t LB_CHUNK = 1u << 22; // bound-table rows (vertices) per query per round
 
 enum Phase : int32_t {
   PH_IDLE = 0,
@@ -81,7 +92,8 @@ struct alignas(16) QCtl {
   unsigned long long stat[12];
   uint32_t done;     // job finished (set by k_control)
   uint32_t final_status;  // gst_status of the finished job
-  uint32_t pad[2];
+  uint32_t infeasible;    // the query groups are not connected
+  uint32_t pad;
 };
 
 // Per-query descriptor; the host rewrites it before each round.
@@ -114,13 +126,23 @@ struct QDev {
   int32_t st, act;
   uint32_t delta, delta_sssp, delta_dp;
   uint32_t par;      // parity of the items in (or entering) the near list
+  uint32_t lb_off;   // bound-table rows (vertices) already computed
 };
 
 struct GraphDev {
   const uint32_t* beg;   // [V+1]
   const uint2* adj;      // [arcs] {neighbour, weight}, each list sorted by (weight, neighbour)
   uint32_t V;
+  const uint32_t* wcut;  // [V][8]: first arc of v with weight > 2^b (b = 0..7), or null
 };
+
+// Upper bound on the end of the arcs of v whose weight is <= lim (the list is
+// sorted by weight): one load of the bucket index instead of a search.
+__device__ __forceinline__ uint32_t arcs_upto(const GraphDev& g, uint32_t v, uint32_t a1, uint32_t lim) {
+  if (g.wcut == nullptr || lim > 128u) return a1;
+  uint32_t b = lim <= 1u ? 0u : 32u - __clz(lim - 1u);  // smallest b with 2^b >= lim
+  return __ldg(g.wcut + (size_t)v * 8 + b);
+}
 
 // DP state flags: 4 bits per state, 8 states per word.  Bits 0 and 1 mark
 // "in the near list" for the two round parities, bit 2 "in the far list".

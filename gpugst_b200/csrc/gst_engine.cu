@@ -29,7 +29,7 @@
 
 namespace gstb {
 __global__ void k_control(QDev*, QCtl*, int, RoundDesc*, uint32_t*);
-__global__ void k_light(const QDev*, const RoundDesc*, const uint32_t*, int, GraphDev);
+__global__ void k_light(const QDev*, RoundDesc*, const uint32_t*, int, GraphDev);
 __global__ void k_heavy(const QDev*, const RoundDesc*, const uint32_t*, int, GraphDev);
 }  // namespace gstb
 
@@ -54,6 +54,7 @@ struct gst_graph {
   uint64_t arcs = 0;
   uint32_t* d_beg = nullptr;
   uint2* d_adj = nullptr;
+  uint32_t* d_wcut = nullptr;  // per vertex: first arc with weight > 2^b, b = 0..7
   // group index (host copy; member lists of a query are built on the host)
   std::vector<uint64_t> grp_ptr;
   std::vector<uint32_t> grp_v;
@@ -93,6 +94,7 @@ struct Job {
   QDev qd{};
   QCtl ctl{};
   int slot = -1;
+  int64_t first_block = 0;  // first round block that runs this job
   gst_status status = GST_OK;
   bool rejected = false;  // failed validation before admission
   bool done = false;
@@ -148,6 +150,10 @@ class Runner {
     CK(cudaSetDevice(g_->device));
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     for (auto& e : ev_) CK(cudaEventCreate(&e));
+    for (auto& e : ev_blk_) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_fin_, cudaEventDisableTiming));
+    for (auto& hh : ev_prof_)
+      for (auto& e : hh) CK(cudaEventCreate(&e));
     cudaMemPool_t pool;
     CK(cudaDeviceGetDefaultMemPool(&pool, g_->device));
     uint64_t thr = ~0ull;
@@ -157,17 +163,38 @@ class Runner {
     cap_num_ = std::max(1u, env_u32("GSTB_SSSP_CAP_NUM", 1));
     cap_den_ = std::max(1u, env_u32("GSTB_SSSP_CAP_DEN", 2));
     max_edges_dev_ = env_u32("GSTB_MAX_TREE_EDGES", 1u << 16);
-    rounds_per_sync_ = std::min(64u, std::max(1u, env_u32("GSTB_ROUNDS_PER_SYNC", 6)));
+    rounds_per_sync_ = std::min(64u, std::max(1u, env_u32("GSTB_ROUNDS_PER_SYNC", 4)));
     max_slots_ = std::min<uint32_t>(MAX_SLOTS - 1, std::max(1u, env_u32("GSTB_MAX_SLOTS", MAX_SLOTS - 1)));
     CK(cudaMalloc(&d_qd_, MAX_SLOTS * sizeof(QDev)));
     CK(cudaMalloc(&d_ctl_, MAX_SLOTS * sizeof(QCtl)));
     CK(cudaMalloc(&d_rd_, sizeof(RoundDesc)));
+    {
+      // hub arc chunk list (k_light -> k_heavy within a round)
+      big_cap_ = std::max(1u << 12, env_u32("GSTB_HUB_CHUNKS", 1u << 20));
+      CK(cudaMalloc(&d_big_, (size_t)big_cap_ * sizeof(uint4)));
+      RoundDesc rd;
+      memset(&rd, 0, sizeof(rd));
+      rd.big = env_u32("GSTB_HUB_SPLIT", 1) ? d_big_ : nullptr;
+      rd.big_cap = big_cap_;
+      rd.hub_min_deg = env_u32("GSTB_HUB_MIN_DEG", 256);
+      rd.hub_min_rest = env_u32("GSTB_HUB_MIN_REST", 128);
+      rd.hub_max_items = env_u32("GSTB_HUB_MAX_ITEMS", 1000000);
+      CK(cudaMemcpy(d_rd_, &rd, sizeof(rd), cudaMemcpyHostToDevice));
+    }
     CK(cudaMalloc(&d_pre_, (size_t)NT * (MAX_SLOTS + 1) * 4));
     CK(cudaMemset(d_qd_, 0, MAX_SLOTS * sizeof(QDev)));
     CK(cudaMemset(d_ctl_, 0, MAX_SLOTS * sizeof(QCtl)));
-    CK(cudaMallocHost(&h_ctl_, MAX_SLOTS * sizeof(QCtl)));
+    CK(cudaMallocHost(&h_ctl_, 2 * MAX_SLOTS * sizeof(QCtl)));
     CK(cudaMallocHost(&h_rd_, sizeof(RoundDesc)));
     CK(cudaMallocHost(&h_qd_, sizeof(QDev)));
+    // pinned staging for admissions (descriptors + member lists) and for the
+    // tree read-back of retired jobs: copies from pinned memory stay
+    // asynchronous, pageable ones would synchronise the stream each time
+    stage_cap_ = (size_t)env_u32("GSTB_STAGE_MB", 32) << 20;
+    CK(cudaMallocHost(&h_stage_, stage_cap_));
+    edge_stage_cap_ = (size_t)env_u32("GSTB_EDGE_STAGE_MB", 16) << 20;
+    CK(cudaMallocHost(&h_edge_stage_, edge_stage_cap_));
+    memset(h_qd_, 0, sizeof(QDev));  // the zero descriptor that frees a slot
     slots_.assign(max_slots_, nullptr);
     int bl = 0, bh = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, k_light, 256, 0));
@@ -184,12 +211,24 @@ class Runner {
     if (d_qd_) cudaFree(d_qd_);
     if (d_ctl_) cudaFree(d_ctl_);
     if (d_rd_) cudaFree(d_rd_);
+    if (d_big_) cudaFree(d_big_);
+    d_big_ = nullptr;
     if (d_pre_) cudaFree(d_pre_);
     if (h_ctl_) cudaFreeHost(h_ctl_);
     if (h_rd_) cudaFreeHost(h_rd_);
     if (h_qd_) cudaFreeHost(h_qd_);
+    if (h_stage_) cudaFreeHost(h_stage_);
+    if (h_edge_stage_) cudaFreeHost(h_edge_stage_);
+    h_stage_ = nullptr;
+    h_edge_stage_ = nullptr;
     for (auto& e : ev_)
       if (e) cudaEventDestroy(e);
+    for (auto& e : ev_blk_)
+      if (e) cudaEventDestroy(e);
+    if (ev_fin_) cudaEventDestroy(ev_fin_);
+    for (auto& hh : ev_prof_)
+      for (auto& e : hh)
+        if (e) cudaEventDestroy(e);
     if (stream_) cudaStreamDestroy(stream_);
     d_qd_ = nullptr;
     d_ctl_ = nullptr;
@@ -235,6 +274,9 @@ class Runner {
   // slot; false if no slot or no device memory is available.
   bool admit(Job* j) {
     if (n_used_ >= max_slots_) return false;
+    const size_t need = align_up(sizeof(QDev), 64) + align_up(sizeof(QCtl), 64) + align_up(j->members.size() * 4, 64);
+    const int sh = (int)(next_block_ & 1);  // staging half of the block this job starts in
+    if (stage_off_[sh] + need > stage_cap_ / 2) return false;  // staging full until that block has run
     void* p = nullptr;
     if (cudaMallocAsync(&p, j->bytes, stream_) != cudaSuccess) {
       cudaGetLastError();
@@ -288,11 +330,19 @@ class Runner {
     cudaMemsetAsync(q.dist, 0xFF, (size_t)g_->V * 8 * 4, stream_);
     cudaMemsetAsync(q.dflag, 0, L.sflag - L.dflag, stream_);
     cudaMemsetAsync(q.sflag, 0, L.qbuf - L.sflag, stream_);
-    cudaMemcpyAsync((void*)q.members, j->members.data(), j->members.size() * 4, cudaMemcpyHostToDevice, stream_);
-    // the descriptors are copied from pageable host memory: the call returns
-    // once the source has been staged, so the job's own copies may be reused
-    cudaMemcpyAsync(d_qd_ + slot, &q, sizeof(QDev), cudaMemcpyHostToDevice, stream_);
-    cudaMemcpyAsync(d_ctl_ + slot, &j->ctl, sizeof(QCtl), cudaMemcpyHostToDevice, stream_);
+    // stage the member list and both descriptors in pinned memory; it is not
+    // reused before the stream synchronises at the end of the next round block
+    char* st = h_stage_ + (size_t)sh * (stage_cap_ / 2) + stage_off_[sh];
+    memcpy(st, &q, sizeof(QDev));
+    char* stc = st + align_up(sizeof(QDev), 64);
+    memcpy(stc, &j->ctl, sizeof(QCtl));
+    char* stm = stc + align_up(sizeof(QCtl), 64);
+    memcpy(stm, j->members.data(), j->members.size() * 4);
+    stage_off_[sh] += need;
+    j->first_block = next_block_;
+    cudaMemcpyAsync((void*)q.members, stm, j->members.size() * 4, cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(d_qd_ + slot, st, sizeof(QDev), cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(d_ctl_ + slot, stc, sizeof(QCtl), cudaMemcpyHostToDevice, stream_);
     slots_[slot] = j;
     n_used_++;
     nslots_hi_ = std::max<uint32_t>(nslots_hi_, (uint32_t)slot + 1);
@@ -309,91 +359,146 @@ class Runner {
 
   // Run rounds until no admitted job is left and admit_more() adds none.
   // `on_done` is called for every finished job (after its results are copied).
+  // Run rounds until no admitted job is left and admit_more() adds none.
+  // `on_done` is called for every finished job (after its results are copied).
+  //
+  // Round blocks are pipelined: block b+1 is launched before the host looks
+  // at block b's control blocks, so the GPU keeps working while the host
+  // retires finished queries and stages new ones.  Everything the host
+  // enqueues (admissions, tree copies, slot clears, frees) is stream-ordered
+  // after the block in flight; staging buffers alternate between two halves.
   template <class AdmitFn, class DoneFn>
   gst_status run(AdmitFn&& admit_more, DoneFn&& on_done) {
     CK(cudaEventRecord(ev_[0], stream_));
+    int64_t inflight = -1;  // id of the block launched but not yet examined
+    std::vector<Job*> fin;  // retired jobs whose tree copies are in flight
+    std::vector<size_t> fin_off;
+    int fin_half = 0;
     for (;;) {
       admit_more();
-      if (n_used_ == 0) {
-        CK(cudaEventRecord(ev_[1], stream_));
-        CK(cudaEventSynchronize(ev_[1]));
-        float ms = 0;
-        CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
-        last_call_ms_ = ms;
-        return GST_OK;
+      int64_t launched = -1;
+      if (n_used_ > 0) {
+        gst_status st = launch_block(rounds_per_sync_);
+        if (st != GST_OK) return st;
+        launched = next_block_++;
       }
-      gst_status st = rounds(rounds_per_sync_);
-      if (st != GST_OK) return st;
-      st = retire(on_done);
-      if (st != GST_OK) return st;
-    }
-  }
-
- private:
-  gst_status rounds(uint32_t R) {
-    GraphDev gd{g_->d_beg, g_->d_adj, g_->V};
-    const int ns = (int)nslots_hi_;
-    const unsigned light_grid = light_grid_, heavy_grid = heavy_grid_;
-    const bool prof = g_->profile;
-    for (uint32_t r = 0; r < R; r++) {
-      k_control<<<1, 1024, 0, stream_>>>(d_qd_, d_ctl_, ns, d_rd_, d_pre_);
-      if (prof) CK(cudaEventRecord(ev_[2 + 3 * r], stream_));
-      k_light<<<light_grid, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
-      if (prof) CK(cudaEventRecord(ev_[3 + 3 * r], stream_));
-      k_heavy<<<heavy_grid, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
-      if (prof) CK(cudaEventRecord(ev_[4 + 3 * r], stream_));
-    }
-    CK(cudaGetLastError());
-    g_->launches += 3ull * R;
-    CK(cudaMemcpyAsync(h_ctl_, d_ctl_, (size_t)ns * sizeof(QCtl), cudaMemcpyDeviceToHost, stream_));
-    CK(cudaStreamSynchronize(stream_));
-    if (prof) {
-      for (uint32_t r = 0; r < R; r++) {
-        float a = 0, b = 0;
-        CK(cudaEventElapsedTime(&a, ev_[2 + 3 * r], ev_[3 + 3 * r]));
-        CK(cudaEventElapsedTime(&b, ev_[3 + 3 * r], ev_[4 + 3 * r]));
-        g_->prof_light_ms += a;
-        g_->prof_heavy_ms += b;
-        g_->prof_rounds++;
+      if (!fin.empty()) {
+        CK(cudaEventSynchronize(ev_fin_));
+        finalize(fin, fin_off, fin_half, on_done);
       }
+      if (inflight >= 0) {
+        const int h = (int)(inflight & 1);
+        CK(cudaEventSynchronize(ev_blk_[h]));
+        stage_off_[h] = 0;  // admissions staged for this block have been copied
+        if (g_->profile) accumulate_profile(h);
+        gst_status st = detect_done(inflight, fin, fin_off);
+        if (st != GST_OK) return st;
+        fin_half = h;
+        if (!fin.empty()) CK(cudaEventRecord(ev_fin_, stream_));
+      }
+      inflight = launched;
+      if (inflight < 0 && n_used_ == 0 && fin.empty()) break;
     }
+    CK(cudaEventRecord(ev_[1], stream_));
+    CK(cudaEventSynchronize(ev_[1]));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
+    last_call_ms_ = ms;
     return GST_OK;
   }
 
-  template <class DoneFn>
-  gst_status retire(DoneFn&& on_done) {
-    std::vector<Job*> fin;
-    for (uint32_t s = 0; s < nslots_hi_; s++) {
+ private:
+  gst_status launch_block(uint32_t R) {
+    GraphDev gd{g_->d_beg, g_->d_adj, g_->V, g_->d_wcut};
+    const int ns = (int)nslots_hi_;
+    const unsigned light_grid = light_grid_, heavy_grid = heavy_grid_;
+    const int h = (int)(next_block_ & 1);
+    const bool prof = g_->profile;
+    cudaEvent_t* pe = ev_prof_[h];
+    for (uint32_t r = 0; r < R; r++) {
+      k_control<<<1, 1024, 0, stream_>>>(d_qd_, d_ctl_, ns, d_rd_, d_pre_);
+      if (prof) CK(cudaEventRecord(pe[3 * r], stream_));
+      k_light<<<light_grid, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
+      if (prof) CK(cudaEventRecord(pe[3 * r + 1], stream_));
+      k_heavy<<<heavy_grid, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
+      if (prof) CK(cudaEventRecord(pe[3 * r + 2], stream_));
+    }
+    CK(cudaGetLastError());
+    prof_rounds_[h] = prof ? R : 0;
+    g_->launches += 3ull * R;
+    blk_slots_[h] = (uint32_t)ns;
+    CK(cudaMemcpyAsync(h_ctl_ + (size_t)h * MAX_SLOTS, d_ctl_, (size_t)ns * sizeof(QCtl), cudaMemcpyDeviceToHost,
+                       stream_));
+    CK(cudaEventRecord(ev_blk_[h], stream_));
+    return GST_OK;
+  }
+
+  void accumulate_profile(int h) {
+    for (uint32_t r = 0; r < prof_rounds_[h]; r++) {
+      float a = 0, b = 0;
+      cudaEventElapsedTime(&a, ev_prof_[h][3 * r], ev_prof_[h][3 * r + 1]);
+      cudaEventElapsedTime(&b, ev_prof_[h][3 * r + 1], ev_prof_[h][3 * r + 2]);
+      g_->prof_light_ms += a;
+      g_->prof_heavy_ms += b;
+      g_->prof_rounds++;
+    }
+  }
+
+  // Jobs that block `blk` saw finish: queue their tree copies, free their
+  // workspace and slot (all stream-ordered after the block in flight).
+  gst_status detect_done(int64_t blk, std::vector<Job*>& fin, std::vector<size_t>& fin_off) {
+    const int h = (int)(blk & 1);
+    const QCtl* snap = h_ctl_ + (size_t)h * MAX_SLOTS;
+    char* estage = h_edge_stage_ + (size_t)h * (edge_stage_cap_ / 2);
+    size_t off = 0;
+    for (uint32_t s = 0; s < blk_slots_[h]; s++) {
       Job* j = slots_[s];
-      if (!j || !h_ctl_[s].done) continue;
-      j->ctl = h_ctl_[s];
+      if (!j || j->first_block > blk || !snap[s].done) continue;
+      j->ctl = snap[s];
       j->status = (gst_status)j->ctl.final_status;
+      size_t my = (size_t)-1;
       if (j->status == GST_OK) {
         j->cost = (int32_t)(j->ctl.best_full >> 32);
         j->root = j->ctl.root;
         uint32_t ne = std::min(j->ctl.n_edges, max_edges_dev_);
         j->edges.resize((size_t)ne * 3);
-        if (ne) CK(cudaMemcpyAsync(j->edges.data(), j->qd.out_edges, (size_t)ne * 12, cudaMemcpyDeviceToHost, stream_));
+        if (ne) {
+          if (off + (size_t)ne * 12 <= edge_stage_cap_ / 2) {
+            CK(cudaMemcpyAsync(estage + off, j->qd.out_edges, (size_t)ne * 12, cudaMemcpyDeviceToHost, stream_));
+            my = off;
+            off += align_up((size_t)ne * 12, 16);
+          } else {  // rare: a huge tree, copy it synchronously
+            CK(cudaMemcpy(j->edges.data(), j->qd.out_edges, (size_t)ne * 12, cudaMemcpyDeviceToHost));
+          }
+        }
       }
-      fin.push_back(j);
-    }
-    if (fin.empty()) return GST_OK;
-    CK(cudaStreamSynchronize(stream_));
-    auto now = std::chrono::steady_clock::now();
-    for (Job* j : fin) {
-      // free the slot: a zeroed descriptor is J_FREE for k_control
-      QDev z;
-      memset(&z, 0, sizeof(z));
-      CK(cudaMemcpyAsync(d_qd_ + j->slot, &z, sizeof(QDev), cudaMemcpyHostToDevice, stream_));
-      slots_[j->slot] = nullptr;
-      n_used_--;
+      // free the slot: a zeroed descriptor is J_FREE for k_control (pinned
+      // source, so the copy stays asynchronous)
+      CK(cudaMemcpyAsync(d_qd_ + s, h_qd_, sizeof(QDev), cudaMemcpyHostToDevice, stream_));
       free_job(j);
+      slots_[s] = nullptr;
+      n_used_--;
+      fin.push_back(j);
+      fin_off.push_back(my);
+    }
+    while (nslots_hi_ > 0 && !slots_[nslots_hi_ - 1]) nslots_hi_--;
+    return GST_OK;
+  }
+
+  template <class DoneFn>
+  void finalize(std::vector<Job*>& fin, std::vector<size_t>& fin_off, int half, DoneFn&& on_done) {
+    const char* estage = h_edge_stage_ + (size_t)half * (edge_stage_cap_ / 2);
+    auto now = std::chrono::steady_clock::now();
+    for (size_t i = 0; i < fin.size(); i++) {
+      Job* j = fin[i];
+      if (j->status == GST_OK && !j->edges.empty() && fin_off[i] != (size_t)-1)
+        memcpy(j->edges.data(), estage + fin_off[i], j->edges.size() * 4);
       j->t_done = now;
       j->done = true;
       on_done(j);
     }
-    while (nslots_hi_ > 0 && !slots_[nslots_hi_ - 1]) nslots_hi_--;
-    return GST_OK;
+    fin.clear();
+    fin_off.clear();
   }
 
   gst_graph* g_;
@@ -403,13 +508,22 @@ class Runner {
   QDev* d_qd_ = nullptr;
   QCtl* d_ctl_ = nullptr;
   RoundDesc* d_rd_ = nullptr;
+  uint4* d_big_ = nullptr;
+  uint32_t big_cap_ = 0;
   uint32_t* d_pre_ = nullptr;
   QCtl* h_ctl_ = nullptr;
   RoundDesc* h_rd_ = nullptr;
   QDev* h_qd_ = nullptr;
+  char* h_stage_ = nullptr;
+  char* h_edge_stage_ = nullptr;
+  size_t stage_cap_ = 0, stage_off_[2] = {0, 0}, edge_stage_cap_ = 0;
+  int64_t next_block_ = 0;
+  uint32_t blk_slots_[2] = {0, 0}, prof_rounds_[2] = {0, 0};
+  cudaEvent_t ev_blk_[2] = {nullptr, nullptr}, ev_fin_ = nullptr;
+  cudaEvent_t ev_prof_[2][3 * 64] = {};
   uint32_t delta_sssp_ = 8, delta_dp_ = 2, max_edges_dev_ = 1u << 16;
   uint32_t cap_num_ = 1, cap_den_ = 2, rounds_per_sync_ = 6;
-  cudaEvent_t ev_[2 + 3 * 64] = {};
+  cudaEvent_t ev_[2] = {};
   unsigned light_grid_ = 148 * 4, heavy_grid_ = 148 * 2;
   double last_call_ms_ = 0;
 };
@@ -513,6 +627,33 @@ gst_status gst_graph_create(const uint32_t* beg_pos, const uint32_t* csr, const 
     gst_graph_destroy(g);
     return GST_CUDA_ERROR;
   }
+  {
+    // weight-bucket index: for each vertex the first arc heavier than 2^b
+    std::vector<uint32_t> wc((size_t)V * 8);
+    std::vector<std::thread> tw;
+    for (unsigned t = 0; t < nth; t++) {
+      tw.emplace_back([&, t]() {
+        for (uint32_t v = t; v < V; v += nth) {
+          uint32_t a = beg_pos[v], a1 = beg_pos[v + 1];
+          for (int b = 0; b < 8; b++) {
+            uint32_t th = 1u << b;
+            while (a < a1 && adj[a].y <= th) a++;
+            wc[(size_t)v * 8 + b] = a;
+          }
+        }
+      });
+    }
+    for (auto& x : tw) x.join();
+    if (cudaMalloc(&g->d_wcut, wc.size() * 4) != cudaSuccess) {
+      cudaGetLastError();
+      gst_graph_destroy(g);
+      return GST_OOM;
+    }
+    if (cudaMemcpy(g->d_wcut, wc.data(), wc.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+      gst_graph_destroy(g);
+      return GST_CUDA_ERROR;
+    }
+  }
   *out = g;
   return GST_OK;
 }
@@ -536,6 +677,7 @@ void gst_graph_destroy(gst_graph* g) {
   if (g->runner) delete static_cast<Runner*>(g->runner);
   if (g->d_beg) cudaFree(g->d_beg);
   if (g->d_adj) cudaFree(g->d_adj);
+  if (g->d_wcut) cudaFree(g->d_wcut);
   delete g;
 }
 
@@ -964,7 +1106,7 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   CK(cudaMemcpy(d_qd, &q, sizeof(QDev), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(d_ctl, &c, sizeof(QCtl), cudaMemcpyHostToDevice));
 
-  GraphDev gd{g->d_beg, g->d_adj, g->V};
+  GraphDev gd{g->d_beg, g->d_adj, g->V, g->d_wcut};
   const unsigned light_grid = (unsigned)g->num_sms * 4, heavy_grid = (unsigned)g->num_sms * 2;
   const uint32_t R = 6;
   const uint64_t max_rounds = 1ull << 22;

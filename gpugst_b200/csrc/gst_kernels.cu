@@ -169,7 +169,7 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
   // CPUNONHOP.h:820; exact for the unbounded problem, see DESIGN)
   if (2ull * c <= best) {
     uint32_t lim = best - c;
-    uint32_t a0 = __ldg(g.beg + v), a1 = __ldg(g.beg + v + 1);
+    uint32_t a0 = __ldg(g.beg + v), a1 = arcs_upto(g, v, __ldg(g.beg + v + 1), lim);
     for (uint32_t base = a0; base < a1; base += 32) {
       uint32_t a = base + lane;
       bool in = a < a1;
@@ -276,7 +276,7 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
   uint32_t scanned = 0, upd = 0;
   if (d < (uint32_t)D) {  // grow d -> d+1 (CPUHOP.h:192-206)
     uint32_t lim = best - c;
-    uint32_t a0 = __ldg(g.beg + v), a1 = __ldg(g.beg + v + 1);
+    uint32_t a0 = __ldg(g.beg + v), a1 = arcs_upto(g, v, __ldg(g.beg + v + 1), lim);
     for (uint32_t base = a0; base < a1; base += 32) {
       uint32_t a = base + lane;
       bool in = a < a1;
@@ -417,7 +417,8 @@ __device__ __forceinline__ void sssp_flush(SsspCounters& sc, uint32_t sl) {
 }
 
 __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restrict__ pre, int nslots,
-                          uint32_t total, uint32_t task, const GraphDev& g, uint32_t lane, SsspCounters& sc) {
+                          uint32_t total, uint32_t task, const GraphDev& g, uint32_t lane, SsspCounters& sc,
+                          RoundDesc* __restrict__ rd) {
   const unsigned FULL = 0xFFFFFFFFu;
   const uint32_t sub = lane >> 3, sl = lane & 7u, gbase = lane & ~7u;
   const uint32_t it = task * 4u + sub;
@@ -483,7 +484,8 @@ __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restric
   for (int t = 0; t < KMAX; t++) d[t] = __shfl_sync(FULL, dj, gbase + t);
   const bool active = rm != 0;
   const uint32_t lim = active ? capb - dmin : 0u;
-  const uint32_t a0 = active ? __ldg(g.beg + v) : 0u, a1 = active ? __ldg(g.beg + v + 1) : 0u;
+  const uint32_t a0 = active ? __ldg(g.beg + v) : 0u;
+  const uint32_t a1 = active ? arcs_upto(g, v, __ldg(g.beg + v + 1), lim) : 0u;
   if (active && sl == 0) sc.items++;
   const uint32_t thi = valid ? q.theta_hi : 0u;
   uint32_t* pnext = valid ? q.sflag + (size_t)(q.par ^ 1u) * V : nullptr;
@@ -525,6 +527,100 @@ __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restric
     append_multi(takeF, arc.x, false, q, slot, lane, sc.enq);
     unsigned stop = __ballot_sync(FULL, over || (more && a + 1 >= a1));
     if ((stop >> gbase) & 0xFFu) done = true;  // sorted by weight: the rest is heavier
+    if (off == 0) {
+      // hub: many arcs left under the limit -> hand them to k_heavy in chunks
+      // of HUB_CHUNK arcs, one warp each, instead of 8 lanes walking them all
+      bool hub = !done && a1 - a0 >= rd->hub_min_deg && rd->hub_on;
+      uint32_t cut = 0, nch = 0, base = 0;
+      if (hub && sl == 0) {
+        cut = a1;  // already cut to the weight bucket of the limit
+        nch = (cut - (a0 + 8) + HUB_CHUNK - 1) / HUB_CHUNK;
+        if (rd->big == nullptr || cut - (a0 + 8) < rd->hub_min_rest) {
+          nch = 0xFFFFFFFFu;  // chunking disabled: keep walking here
+        } else if (nch > 0) {
+          base = atomicAdd(&rd->n_big, nch);
+          if (base + nch <= rd->big_cap) {
+            for (uint32_t c = 0; c < nch; c++) {
+              uint32_t st = a0 + 8 + c * HUB_CHUNK;
+              rd->big[base + c] = make_uint4(slot | (rm << 16), v, st, min(st + HUB_CHUNK, cut));
+            }
+          } else {
+            nch = 0xFFFFFFFFu;  // no room: keep walking here
+          }
+        }
+      }
+      nch = __shfl_sync(FULL, nch, gbase);
+      if (hub && nch != 0xFFFFFFFFu) done = true;
+    }
+  }
+}
+
+// One hub chunk (k_heavy, one warp): relax arcs [first, end) of vertex v for
+// the pending groups recorded by k_light.  Same relaxation as sssp_task.
+__device__ void hub_chunk(const QDev* __restrict__ qd, const uint4 item, const GraphDev& g, uint32_t lane) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  const uint32_t slot = item.x & 0xFFFFu, rm = item.x >> 16, v = item.y;
+  const QDev& q = qd[slot];
+  const uint32_t V = q.nv;
+  const uint32_t dj = lane < 8 ? ld_cg(q.dist + (size_t)v * 8 + lane) : INF32;
+  uint32_t d[KMAX];
+#pragma unroll
+  for (int t = 0; t < KMAX; t++) d[t] = __shfl_sync(FULL, dj, t);
+  const uint32_t best = __shfl_sync(FULL, ld_cg(&q.ctl->best), 0);
+  const uint32_t capb = (uint32_t)((unsigned long long)best * q.cap_num / q.cap_den);
+  uint32_t dmin = INF32;
+#pragma unroll
+  for (int t = 0; t < KMAX; t++)
+    if ((rm >> t) & 1u) dmin = min(dmin, d[t]);
+  if (dmin > capb) return;
+  const uint32_t lim = capb - dmin, thi = q.theta_hi;
+  uint32_t* pnext = q.sflag + (size_t)(q.par ^ 1u) * V;
+  uint32_t* pfar = q.sflag + (size_t)2 * V;
+  uint32_t n_arcs = 0, n_upd = 0, n_enq = 0;
+  for (uint32_t a0 = item.z; a0 < item.w; a0 += 32) {
+    uint32_t a = a0 + lane;
+    bool in = a < item.w;
+    uint2 arc = in ? __ldg(g.adj + a) : make_uint2(0, 0xFFFFFFFFu);
+    bool over = in && arc.y > lim;
+    bool takeN = false, takeF = false;
+    if (in && !over) {
+      n_arcs++;
+      const uint32_t u = arc.x;
+      const uint4* row = reinterpret_cast<const uint4*>(q.dist + (size_t)u * 8);
+      uint4 ra = __ldcg(row), rb = __ldcg(row + 1);
+      uint32_t du[8] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
+      uint32_t nn = 0, nf = 0;
+#pragma unroll
+      for (int t = 0; t < KMAX; t++) {
+        if ((rm >> t) & 1u) {
+          uint32_t nd = d[t] + arc.y;
+          if (nd <= capb && nd < du[t]) {
+            atomicMin(q.dist + (size_t)u * 8 + t, nd);
+            if (nd < thi)
+              nn |= 1u << t;
+            else
+              nf |= 1u << t;
+            n_upd++;
+          }
+        }
+      }
+      if (nn) takeN = atomicOr(pnext + u, nn) == 0u;
+      if (nf) takeF = atomicOr(pfar + u, nf) == 0u;
+    }
+    append_multi(takeN, arc.x, true, q, slot, lane, n_enq);
+    append_multi(takeF, arc.x, false, q, slot, lane, n_enq);
+    if (__any_sync(FULL, over)) break;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    n_arcs += __shfl_xor_sync(FULL, n_arcs, o);
+    n_upd += __shfl_xor_sync(FULL, n_upd, o);
+    n_enq += __shfl_xor_sync(FULL, n_enq, o);
+  }
+  if (lane == 0) {
+    if (n_arcs) atomicAdd(&q.ctl->stat[ST_SSSP_ARCS], (unsigned long long)n_arcs);
+    if (n_upd) atomicAdd(&q.ctl->stat[ST_SSSP_UPDATES], (unsigned long long)n_upd);
+    if (n_enq) atomicAdd(&q.ctl->stat[ST_SSSP_ENQ], (unsigned long long)n_enq);
   }
 }
 
@@ -621,6 +717,15 @@ __device__ void tour_warp(const QDev& q, uint32_t lane) {
     for (int j = 0; j < k; j++) atomicMin(&gd[i * 8 + j], min(q.dist[(size_t)v * 8 + j], q.cap1));
   }
   __syncwarp();
+  // With no feasible tree found yet the distance rounds ran without a cap, so
+  // an unreachable pair of groups proves there is no solution at all.
+  if (lane == 0 && ld_cg(&q.ctl->best) == INF32) {
+    bool cut = false;
+    for (int i = 0; i < k; i++)
+      for (int j = 0; j < k; j++)
+        if (i != j && __ldcg(&gd[i * 8 + j]) >= BIG) cut = true;
+    if (cut) q.ctl->infeasible = 1u;
+  }
   const uint32_t nP = (uint32_t)k * K2 * (uint32_t)k;
   for (uint32_t t = lane; t < nP; t += 32) P[t] = BIG;
   __syncwarp();
@@ -647,27 +752,25 @@ __device__ void tour_warp(const QDev& q, uint32_t lane) {
   __syncwarp();
 }
 
-// Lower-bound table of one vertex: lbt[v][X] = lower_bound_comp(d(v), X)
-// for every subset X, saturated to 16 bits (the per-vertex one_label_lb table
-// of the reference, DPQ.cu:174-224, with the tour bounds of
-// CPUNONHOP.h:436-496).  Saturation only lowers a bound, so it stays valid.
-__device__ void lbt_vertex(const QDev& q, uint32_t v) {
+// Lower-bound table row of vertex v: lbt[v][X] = lower_bound_comp(d(v), X)
+// for every subset X (the per-vertex one_label_lb table of the reference,
+// DPQ.cu:174-224, with the tour bounds of CPUNONHOP.h:436-496).  Eight lanes
+// share a vertex and split its subsets.  Saturated to 16 bits, which only
+// lowers a bound.
+__device__ void lbt_row8(const QDev& q, uint32_t v, uint32_t sl) {
   const int k = q.k;
   const uint32_t K2 = 1u << k;
   const uint32_t* P = q.tour;
   const uint32_t* T2 = q.tour + (size_t)k * K2 * k;
   const uint4* row = reinterpret_cast<const uint4*>(q.dist + (size_t)v * 8);
-  uint4 a = __ldcg(row), b = __ldcg(row + 1);
+  uint4 a = __ldg(row), b = __ldg(row + 1);
   uint32_t r[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
   uint32_t dl[KMAX];
 #pragma unroll
   for (int j = 0; j < KMAX; j++) dl[j] = min(r[j], q.cap1);
   unsigned short* out = q.lbt + ((size_t)v << k);
-  out[0] = 0;
-  for (uint32_t X = 1; X < K2; X++) {
-    uint32_t lb = lower_bound_comp(dl, k, X, P, T2);
-    out[X] = (unsigned short)min(lb, 65535u);
-  }
+  for (uint32_t X = sl; X < K2; X += 8)
+    out[X] = X == 0 ? (unsigned short)0 : (unsigned short)min(lower_bound_comp(dl, k, X, P, T2), 65535u);
 }
 
 // Weight of arc (a -> b): linear scan of a's weight-sorted adjacency.
@@ -790,10 +893,12 @@ __device__ __forceinline__ void absorb(QDev& q, QCtl& c) {
       q.n_far = c.n_far2;
       break;
     case A_TOUR:
-      q.st = J_LB;
+      q.st = c.infeasible ? J_EXTRACT : J_LB;  // disconnected groups: straight to "no solution"
       break;
     case A_LB:
-      q.st = J_DPSEED;
+      // the bound table is filled in chunks of LB_CHUNK entries per round
+      q.lb_off += min(q.nv - q.lb_off, LB_CHUNK);
+      if (q.lb_off >= q.nv) q.st = J_DPSEED;
       break;
     case A_DSEED:
       t = q.in_idx; q.in_idx = q.out_idx; q.out_idx = t;
@@ -906,7 +1011,7 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
         case A_DSEED: cnt[T_DSEED] = q.n_members; break;
         case A_SPLIT: cnt[T_SPLIT] = q.n_far; break;
         case A_TOUR: cnt[T_TOUR] = 1; break;
-        case A_LB: cnt[T_LB] = q.nv; break;
+        case A_LB: cnt[T_LB] = min(q.nv - q.lb_off, LB_CHUNK); break;
         case A_EXTRACT: cnt[T_EXTRACT] = 1; break;
         case A_WORK:
           cnt[q.phase == PH_SSSP ? T_SSSP : (q.phase == PH_DP ? T_DP : T_HOP)] = q.n_in;
@@ -950,7 +1055,7 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
     if (tid <= nslots) pre[t * (MAX_SLOTS + 1) + tid] = before;
   }
   if (tid == 0) {
-    const uint32_t per_task[NT] = {32, 32, 32, 1, 1, 4, 32, 1, 1};
+    const uint32_t per_task[NT] = {32, 32, 32, 1, 1, 4, 4, 1, 1};
     uint32_t off = 0;
     for (int t = 0; t < NT; t++) {
       uint32_t tot = wsum[(blockDim.x >> 5) - 1][t];
@@ -965,13 +1070,16 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
     rd->task_off[NT] = off;
     rd->heavy_tasks = off;
     rd->n_live = live_cnt;
+    rd->n_big = 0;
+    // hub chunking pays off only when the round is too small to fill the GPU
+    rd->hub_on = (rd->big != nullptr && rd->items[T_SSSP] < rd->hub_max_items) ? 1u : 0u;
   }
 }
 
 // ---------------------------------------------------------------------------
 // Light round kernel: warp tasks of types T_SPLIT .. T_SSSP.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_light(const QDev* __restrict__ qd, const RoundDesc* __restrict__ rd,
+__global__ void __launch_bounds__(256) k_light(const QDev* __restrict__ qd, RoundDesc* __restrict__ rd,
                                                const uint32_t* __restrict__ pre, int nslots, GraphDev g) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -989,7 +1097,7 @@ __global__ void __launch_bounds__(256) k_light(const QDev* __restrict__ qd, cons
     const uint32_t* P = pre + t * (MAX_SLOTS + 1);
     const uint32_t total = __ldcg(&rd->items[t]);
     if (t == T_SSSP) {
-      sssp_task(qd, s_pre, nslots, total, local, g, lane, sc);
+      sssp_task(qd, s_pre, nslots, total, local, g, lane, sc, rd);
     } else if (t == T_TOUR) {
       tour_warp(qd[find_slot(P, nslots, local)], lane);
     } else if (t == T_EXTRACT) {
@@ -1019,21 +1127,28 @@ __global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, cons
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t ntasks = __ldcg(&rd->heavy_tasks);
-  const uint32_t dp0 = __ldcg(&rd->task_off[T_DP]), hop0 = __ldcg(&rd->task_off[T_HOP]);
-  __shared__ uint32_t s_dp[MAX_SLOTS + 1], s_hop[MAX_SLOTS + 1];
+  // hub arc chunks queued by k_light come first in the task space
+  const uint32_t nbig = rd->big ? min(__ldcg(&rd->n_big), rd->big_cap) : 0u;
+  const uint32_t ntasks = __ldcg(&rd->heavy_tasks) + nbig;
+  const uint32_t dp0 = __ldcg(&rd->task_off[T_DP]) + nbig, hop0 = __ldcg(&rd->task_off[T_HOP]) + nbig;
+  __shared__ uint32_t s_dp[MAX_SLOTS + 1], s_hop[MAX_SLOTS + 1], s_lb[MAX_SLOTS + 1];
   for (int i = threadIdx.x; i <= nslots; i += blockDim.x) {
     s_dp[i] = __ldcg(pre + T_DP * (MAX_SLOTS + 1) + i);
     s_hop[i] = __ldcg(pre + T_HOP * (MAX_SLOTS + 1) + i);
+    s_lb[i] = __ldcg(pre + T_LB * (MAX_SLOTS + 1) + i);
   }
   __syncthreads();
   for (uint32_t task = warp; task < ntasks; task += nwarps) {
-    if (task < dp0) {  // lower-bound table rows, one vertex per lane
-      const uint32_t* P = pre + T_LB * (MAX_SLOTS + 1);
-      uint32_t it = task * 32u + lane;
+    if (task < nbig) {
+      hub_chunk(qd, __ldcg(rd->big + task), g, lane);
+      continue;
+    }
+    if (task < dp0) {  // lower-bound table rows, 8 lanes per vertex
+      uint32_t it = (task - nbig) * 4u + (lane >> 3);
       if (it < __ldcg(&rd->items[T_LB])) {
-        uint32_t slot = find_slot(P, nslots, it);
-        lbt_vertex(qd[slot], it - __ldcg(P + slot));
+        uint32_t slot = find_slot_s(s_lb, nslots, it);
+        const QDev& ql = qd[slot];
+        lbt_row8(ql, ql.lb_off + (it - s_lb[slot]), lane & 7u);
       }
       continue;
     }
