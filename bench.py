@@ -320,7 +320,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
-    from gpugst_b200 import build, engine
+    from gpugst_b200 import build, engine, replicas
     build.build()
     E = engine.Engine.from_instance(g, gr)
 
@@ -366,10 +366,7 @@ def main():
 
     tot_dev = sum(dev_ms)
     tot_wall = sum(wall_ms)
-    if dist:
-        t = torch.tensor([tot_dev, tot_wall], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_dev, tot_wall = float(t[0]), float(t[1])
+    tot_dev, tot_wall = replicas.max_over_ranks([tot_dev, tot_wall], device="cuda")
     nq_all = B * args.steps * world
     value = nq_all / (tot_dev / 1e3)
     e2e_value = nq_all / (tot_wall / 1e3)
@@ -392,8 +389,8 @@ def main():
     per_launch_alg = dom_bytes / max(prof_rounds, 1)
 
     # continuous-batching serving loop (closed loop, `--inflight` requests on the device)
-    S = engine.Server(E, max_inflight=args.inflight)
     n_serve = args.serve
+    S = engine.Server(E, max_inflight=args.inflight) if n_serve > 0 else None
     serve_q = [pool[(rank * 104729 + 7 * i) % len(pool)] for i in range(n_serve)]
     lat_serve = []
     t0 = time.perf_counter()
@@ -414,8 +411,9 @@ def main():
                 S.submit(nxt, serve_q[nxt])
                 nxt += 1
     serve_wall = time.perf_counter() - t0
-    S.close()
-    serve_qps = n_serve / serve_wall
+    if S is not None:
+        S.close()
+    serve_qps = n_serve / serve_wall if n_serve > 0 else None
 
     # plain per-query path (one query per call, gst_query), same workload
     plain_lat, plain_dev = [], []
@@ -425,7 +423,7 @@ def main():
         r = E.query(q)
         plain_lat.append(1e3 * (time.perf_counter() - t0))
         plain_dev.append(r.device_ms)
-    plain_qps = len(plain_lat) / (sum(plain_lat) / 1e3)
+    plain_qps = len(plain_lat) / (sum(plain_lat) / 1e3) if plain_lat else None
 
     def pct(xs, p):
         return float(np.percentile(np.array(xs), p)) if xs else None
@@ -456,7 +454,7 @@ def main():
             "plain_per_query": {"value": plain_qps, "unit": "queries/s", "queries": len(plain_lat),
                                 "device_ms_p50": pct(plain_dev, 50)},
             "batched_vs_plain": value / plain_qps if plain_qps else None,
-            "serve_vs_plain": serve_qps / plain_qps if plain_qps else None,
+            "serve_vs_plain": serve_qps / plain_qps if (plain_qps and serve_qps) else None,
             "serve": {"value": serve_qps, "unit": "queries/s", "inflight": args.inflight, "queries": n_serve,
                       "p50_ms": pct(lat_serve, 50), "p99_ms": pct(lat_serve, 99)},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,

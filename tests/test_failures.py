@@ -1,0 +1,157 @@
+"""Failure detection without a GPU fault: malformed inputs are rejected on the
+host with status codes (no exit(), no device work), and the CLI reports bad
+files.  The checks that need a device handle are marked gpu."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from gpugst_b200 import build, gen, formats
+
+
+@pytest.fixture(scope="module")
+def L():
+    lib = ctypes.CDLL(build.build())
+    vp = ctypes.c_void_p
+    lib.gst_graph_create.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(vp)]
+    lib.gst_graph_create.restype = ctypes.c_int
+    return lib
+
+
+def _create(L, beg, csr, w, V=None, arcs=None):
+    beg = np.ascontiguousarray(beg, np.uint32)
+    csr = np.ascontiguousarray(csr, np.uint32)
+    w = np.ascontiguousarray(w, np.int32)
+    h = ctypes.c_void_p()
+    st = L.gst_graph_create(beg.ctypes.data, csr.ctypes.data if len(csr) else None, w.ctypes.data if len(w) else None,
+                            len(beg) - 1 if V is None else V, len(csr) if arcs is None else arcs, ctypes.byref(h))
+    return st, h
+
+
+def test_graph_create_rejects_malformed_csr(L):
+    BAD = 2
+    # beg_pos not monotone
+    assert _create(L, [0, 2, 1, 2], [1, 2], [1, 1])[0] == BAD
+    # neighbour out of range
+    assert _create(L, [0, 1, 2], [1, 7], [3, 3])[0] == BAD
+    # non-positive weight
+    assert _create(L, [0, 1, 2], [1, 0], [0, 0])[0] == BAD
+    # arcs disagree with beg_pos[V]
+    assert _create(L, [0, 1, 2], [1, 0], [2, 2], arcs=3)[0] == BAD
+    # no vertices
+    assert _create(L, [0], [], [], V=0)[0] == BAD
+
+
+def test_cli_usage_and_missing_files(tmp_path):
+    cli = build.build_cli()
+    r = subprocess.run([cli], capture_output=True, text=True)
+    assert r.returncode == 2 and "usage" in r.stderr
+    r = subprocess.run([cli, "2", str(tmp_path) + "/", "nope", "3", "0", "1"], capture_output=True, text=True)
+    assert r.returncode == 1 and "cannot read the graph" in r.stderr
+
+
+def test_python_binding_fails_loudly_without_library(monkeypatch, tmp_path):
+    from gpugst_b200 import engine
+    monkeypatch.setattr(engine, "LIB_PATH", str(tmp_path / "missing.so"))
+    monkeypatch.setattr(engine, "_lib", None)
+    with pytest.raises(RuntimeError):
+        engine.lib()
+
+
+def test_format_roundtrip(tmp_path):
+    g, gr = gen.small_instance(60, 200, 12, 5, seed=3)
+    q = gen.queries(gr.n_groups, 4, 3, seed=4)
+    formats.write_dataset(str(tmp_path), "x", g, gr, {3: q})
+    g2 = formats.read_in(str(tmp_path / "x.in"))
+    gr2 = formats.read_g(str(tmp_path / "x.g"))
+    assert (g2.beg_pos == g.beg_pos).all() and (g2.csr == g.csr).all() and (g2.weight == g.weight).all()
+    assert (gr2.ptr == gr.ptr).all() and (gr2.members == gr.members).all()
+    q2 = formats.read_queries(str(tmp_path / "x3.csv"))
+    assert [list(x) for x in q2] == [list(x) for x in q]
+    formats.write_bin(str(tmp_path / "x"), g)
+    g3 = formats.read_bin(str(tmp_path / "x"))
+    assert (g3.csr == g.csr).all() and (g3.weight == g.weight).all()
+
+
+@pytest.mark.gpu
+def test_groups_set_rejects_bad_members(gst_lib):
+    eng = gst_lib
+    g, gr = gen.small_instance(30, 80, 6, 3, seed=5)
+    E = eng.Engine(g.beg_pos, g.csr, g.weight)
+    with pytest.raises(eng.GstError):
+        E.set_groups(np.array([0, 1], np.uint64), np.array([99], np.uint32))  # vertex out of range
+    with pytest.raises(eng.GstError):
+        E.set_groups(np.array([1, 1], np.uint64), np.array([0], np.uint32))   # ptr[0] != 0
+    E.close()
+
+
+@pytest.mark.gpu
+def test_queue_overflow_is_reported(tmp_path):
+    """A frontier larger than GSTB_QUEUE_CAP returns GST_QUEUE_OVERFLOW instead
+    of writing out of bounds (run in a child process with a tiny capacity)."""
+    code = r'''
+import sys, numpy as np
+sys.path.insert(0, %r)
+from gpugst_b200 import engine, gen
+g, gr = gen.small_instance(3000, 30000, 200, 20, seed=8)
+E = engine.Engine.from_instance(g, gr)
+r = E.query(np.array([0, 1, 2, 3], np.uint32))
+print("STATUS", r.status)
+''' % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))),)
+    env = dict(os.environ, GSTB_QUEUE_CAP="1")
+    out = subprocess.run(["python", "-c", code], capture_output=True, text=True, env=env, timeout=300)
+    assert "STATUS 6" in out.stdout, out.stdout + out.stderr
+
+
+@pytest.mark.gpu
+def test_serve_with_tiny_budget_admits_one_at_a_time(gst_lib):
+    """An HBM budget below one workspace still serves every request (one at a
+    time) with the same results."""
+    import time
+    eng = gst_lib
+    g, gr, qs = gen.config1()
+    E = eng.Engine.from_instance(g, gr)
+    want = [E.query(q).cost for q in qs[3][:6]]
+    S = eng.Server(E, hbm_budget=1, max_inflight=8)
+    for i, q in enumerate(qs[3][:6]):
+        assert S.submit(i, q) == eng.GST_OK
+    got = {}
+    t0 = time.time()
+    while len(got) < 6 and time.time() - t0 < 60:
+        for rid, r in S.poll():
+            got[rid] = r.cost
+        time.sleep(0.001)
+    S.close()
+    E.close()
+    assert [got[i] for i in range(6)] == want
+
+
+@pytest.mark.gpu
+def test_cli_matches_oracle(tmp_path, oracle_mod):
+    O = oracle_mod
+    g, gr, qs = gen.config1()
+    formats.write_dataset(str(tmp_path), "c1", g, gr, {3: qs[3][:10]})
+    cli = build.build_cli()
+    r = subprocess.run([cli, "2", str(tmp_path) + "/", "c1", "3", "0", "9"], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    rows = open(tmp_path / "result" / "exp_GPU1_nonHop_c1_T3_0-9.csv").read().strip().splitlines()
+    assert rows[0].startswith("task_ID,task,GPU1_nonHop_time,GPU_nonHop_cost")
+    costs = [int(x.split(",")[3]) for x in rows[1:]]
+    assert costs == [O.prunedpp(g, gr, q, 0).cost for q in qs[3][:10]]
+    # hop-bounded argv form and the int64 .bin CSR
+    formats.write_bin(str(tmp_path / "c1b"), g)
+    formats.write_g(str(tmp_path / "c1b.g"), gr)
+    formats.write_queries(str(tmp_path / "c1b3.csv"), qs[3][:5])
+    r = subprocess.run([cli, "2", str(tmp_path) + "/", "c1b", "3", "4", "0", "4"], capture_output=True, text=True,
+                       timeout=300, env=dict(os.environ, GSTB_CLI_BATCH="1"))
+    assert r.returncode == 0, r.stderr
+    rows = open(tmp_path / "result" / "exp_GPU1_Hop_c1b_T3_D4_0-4.csv").read().strip().splitlines()
+    costs = [int(x.split(",")[3]) for x in rows[1:]]
+    want = []
+    for q in qs[3][:5]:
+        h = O.hop(g, gr, q, 4)
+        want.append(h.cost if h.status == 0 else 0)
+    assert costs == want
