@@ -63,11 +63,22 @@ def csr_from_edges(V: int, u: np.ndarray, v: np.ndarray, w: np.ndarray) -> Graph
     u = np.asarray(u, dtype=np.int64)
     v = np.asarray(v, dtype=np.int64)
     w = np.asarray(w, dtype=np.int32)
-    src = np.concatenate([u, v])
-    dst = np.concatenate([v, u])
-    ww = np.concatenate([w, w])
-    order = np.lexsort((dst, src))
-    src, dst, ww = src[order], dst[order], ww[order]
+    if len(w) and 0 <= int(w.min()) and int(w.max()) < 128 and V < (1 << 28):
+        # one sort of packed (src, dst, weight) keys instead of a two-key lexsort
+        key = np.concatenate([u * V + v, v * V + u])
+        key *= 128
+        key += np.concatenate([w, w]).astype(np.int64)
+        key.sort()
+        ww = (key % 128).astype(np.int32)
+        key //= 128
+        src = key // V
+        dst = key % V
+    else:
+        src = np.concatenate([u, v])
+        dst = np.concatenate([v, u])
+        ww = np.concatenate([w, w])
+        order = np.lexsort((dst, src))
+        src, dst, ww = src[order], dst[order], ww[order]
     counts = np.bincount(src, minlength=V)
     beg = np.zeros(V + 1, dtype=np.uint64)
     np.cumsum(counts, out=beg[1:])
@@ -76,12 +87,46 @@ def csr_from_edges(V: int, u: np.ndarray, v: np.ndarray, w: np.ndarray) -> Graph
     return Graph(V, beg.astype(np.uint32), dst.astype(np.uint32), ww)
 
 
+def _take_sorted(keys: np.ndarray, E: int, rng) -> np.ndarray:
+    """E keys chosen uniformly at random (linear-time selection), sorted."""
+    if len(keys) <= E:
+        return keys
+    pri = rng.random(len(keys))
+    idx = np.argpartition(pri, E)[:E]
+    out = keys[idx]
+    out.sort()
+    return out
+
+
+def _sample_endpoints(cdf: np.ndarray, n: int, rng) -> np.ndarray:
+    """n vertices drawn from the distribution `cdf`, in random order.  The
+    uniforms are sorted before the search (cache-friendly), then the result
+    is shuffled; the multiset drawn is the same as with unsorted uniforms."""
+    x = rng.random(n)
+    x.sort()
+    a = np.searchsorted(cdf, x, side="right")
+    rng.shuffle(a)
+    return np.minimum(a, len(cdf) - 1)
+
+
+def _sorted_unique(x: np.ndarray) -> np.ndarray:
+    """Sorted distinct values (sort + mask; faster than np.unique on large
+    integer arrays with mostly distinct values)."""
+    x = np.sort(x)
+    if len(x) == 0:
+        return x
+    keep = np.empty(len(x), dtype=bool)
+    keep[0] = True
+    np.not_equal(x[1:], x[:-1], out=keep[1:])
+    return x[keep]
+
+
 def _unique_edges(V: int, a: np.ndarray, b: np.ndarray) -> np.ndarray:
     keep = a != b
     a, b = a[keep], b[keep]
     lo = np.minimum(a, b).astype(np.int64)
     hi = np.maximum(a, b).astype(np.int64)
-    return np.unique(lo * V + hi)
+    return _sorted_unique(lo * V + hi)
 
 
 def chung_lu(V: int, E: int, gamma: float, seed: int, wmax: int = 100) -> Graph:
@@ -112,16 +157,14 @@ def chung_lu(V: int, E: int, gamma: float, seed: int, wmax: int = 100) -> Graph:
     need = E
     while True:
         n = int(need * 1.15) + 1024
-        a = np.searchsorted(cdf, rng.random(n), side="right")
-        b = np.searchsorted(cdf, rng.random(n), side="right")
-        a = np.minimum(a, V - 1)
-        b = np.minimum(b, V - 1)
-        keys = np.union1d(keys, _unique_edges(V, a, b))
+        a = _sample_endpoints(cdf, n, rng)
+        b = _sample_endpoints(cdf, n, rng)
+        new = _unique_edges(V, a, b)
+        keys = new if len(keys) == 0 else _sorted_unique(np.concatenate([keys, new]))
         if len(keys) >= E:
             break
         need = E - len(keys)
-    if len(keys) > E:
-        keys = np.sort(rng.permutation(keys)[:E])
+    keys = _take_sorted(keys, E, rng)
     u = keys // V
     v = keys % V
     w = rng.integers(1, wmax + 1, size=len(keys), dtype=np.int32)
@@ -144,12 +187,12 @@ def rmat(scale: int, E: int, seed: int, a=0.57, b=0.19, c=0.19, wmax: int = 100)
             dbit = (((r >= a) & (r < a + b)) | (r >= a + b + c)).astype(np.int64)  # b, d
             src = (src << 1) | sbit
             dst = (dst << 1) | dbit
-        keys = np.union1d(keys, _unique_edges(V, perm[src], perm[dst]))
+        new = _unique_edges(V, perm[src], perm[dst])
+        keys = new if len(keys) == 0 else _sorted_unique(np.concatenate([keys, new]))
         if len(keys) >= E:
             break
         need = E - len(keys)
-    if len(keys) > E:
-        keys = np.sort(rng.permutation(keys)[:E])
+    keys = _take_sorted(keys, E, rng)
     u = keys // V
     v = keys % V
     w = rng.integers(1, wmax + 1, size=len(keys), dtype=np.int32)
@@ -226,6 +269,28 @@ def config3(seed: int = 3, n_per_cell: int = 100):
     qs = {(k, D): queries(gr.n_groups, n_per_cell, k, seed=3000 + 100 * seed + 10 * k + D)
           for k in (3, 4, 5) for D in (2, 3, 4)}
     return g, gr, qs
+
+
+def config4(seed: int = 4, n_queries: int = 1024):
+    """V=3M, E=117M Chung-Lu (gamma 2.1); 1M Zipf(1.3) groups in [1,500];
+    1,024 queries, k uniform in {3,4,5,6}, half with D uniform in {2,3,4}."""
+    g = chung_lu(3_000_000, 117_000_000, 2.1, seed=1000 + seed)
+    gr = zipf_groups(g.V, 1_000_000, 1.3, 500, seed=2000 + seed)
+    rng = np.random.default_rng(3000 + seed)
+    qs, Ds = [], []
+    for _ in range(n_queries):
+        k = int(rng.integers(3, 7))
+        qs.append(rng.choice(gr.n_groups, size=k, replace=False).astype(np.uint32))
+        Ds.append(int(rng.choice([2, 3, 4])) if rng.random() < 0.5 else -1)
+    return g, gr, qs, Ds
+
+
+def poisson_arrivals(rate: float, duration: float, seed: int) -> np.ndarray:
+    """Arrival times (seconds) of a Poisson process of the given rate."""
+    rng = np.random.default_rng(seed)
+    n = int(rate * duration * 1.5) + 16
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    return t[t < duration]
 
 
 def small_instance(V: int, E: int, n_groups: int, smax: int, seed: int, gamma: float = 2.5):
