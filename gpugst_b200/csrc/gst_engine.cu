@@ -95,6 +95,8 @@ struct Job {
   QCtl ctl{};
   int slot = -1;
   int64_t first_block = 0;  // first round block that runs this job
+  uint64_t cap_req = 0;      // frontier capacity after an overflow retry (0 = default)
+  uint32_t retries = 0;      // runs repeated after GST_QUEUE_OVERFLOW
   gst_status status = GST_OK;
   bool rejected = false;  // failed validation before admission
   bool done = false;
@@ -113,12 +115,15 @@ struct Layout {
   uint32_t cap;
 };
 
-Layout layout_for(const gst_graph* g, int k, int nd, size_t n_members, uint32_t max_edges) {
+// cap_req > 0 asks for a frontier-list capacity of that many items (a query
+// retried after GST_QUEUE_OVERFLOW); 0 takes the default.
+Layout layout_for(const gst_graph* g, int k, int nd, size_t n_members, uint32_t max_edges, uint64_t cap_req = 0) {
   Layout L{};
   uint64_t WT = (uint64_t)(1u << k) * nd;
   uint64_t states = (uint64_t)g->V * WT;
   uint64_t caplim = env_u32("GSTB_QUEUE_CAP", 1u << 25);
   uint64_t cap = std::max<uint64_t>(std::min<uint64_t>(states, caplim), std::min<uint64_t>((uint64_t)g->V * k, caplim));
+  if (cap_req) cap = cap_req;
   cap = std::max<uint64_t>(cap, 1024);
   L.cap = (uint32_t)cap;
   size_t o = 0;
@@ -261,7 +266,7 @@ class Runner {
       for (uint64_t t = g_->grp_ptr[gi]; t < g_->grp_ptr[gi + 1]; t++)
         j->members.push_back(g_->grp_v[t] * 8u + (uint32_t)i);
     }
-    Layout L = layout_for(g_, j->k, j->nd, j->members.size(), max_edges_dev_);
+    Layout L = layout_for(g_, j->k, j->nd, j->members.size(), max_edges_dev_, j->cap_req);
     j->table_bytes = (size_t)g_->V * j->WT * 8;
     j->bytes = L.total;
     return GST_OK;
@@ -290,7 +295,7 @@ class Runner {
       }
     j->mem = (char*)p;
     j->slot = slot;
-    Layout L = layout_for(g_, j->k, j->nd, j->members.size(), max_edges_dev_);
+    Layout L = layout_for(g_, j->k, j->nd, j->members.size(), max_edges_dev_, j->cap_req);
     QDev& q = j->qd;
     memset(&q, 0, sizeof(q));
     q.table = (unsigned long long*)(j->mem + L.table);
@@ -359,8 +364,6 @@ class Runner {
 
   // Run rounds until no admitted job is left and admit_more() adds none.
   // `on_done` is called for every finished job (after its results are copied).
-  // Run rounds until no admitted job is left and admit_more() adds none.
-  // `on_done` is called for every finished job (after its results are copied).
   //
   // Round blocks are pipelined: block b+1 is launched before the host looks
   // at block b's control blocks, so the GPU keeps working while the host
@@ -375,6 +378,20 @@ class Runner {
     std::vector<size_t> fin_off;
     int fin_half = 0;
     for (;;) {
+      // queries retried with larger frontier lists go first
+      while (!retry_.empty() && has_free_slot()) {
+        Job* j = retry_.front();
+        if (!admit(j)) {
+          if (n_used_ > 0) break;  // wait for memory
+          j->status = GST_OOM;     // does not fit even alone
+          j->done = true;
+          j->t_done = std::chrono::steady_clock::now();
+          retry_.pop_front();
+          on_done(j);
+          continue;
+        }
+        retry_.pop_front();
+      }
       admit_more();
       int64_t launched = -1;
       if (n_used_ > 0) {
@@ -397,7 +414,7 @@ class Runner {
         if (!fin.empty()) CK(cudaEventRecord(ev_fin_, stream_));
       }
       inflight = launched;
-      if (inflight < 0 && n_used_ == 0 && fin.empty()) break;
+      if (inflight < 0 && n_used_ == 0 && fin.empty() && retry_.empty()) break;
     }
     CK(cudaEventRecord(ev_[1], stream_));
     CK(cudaEventSynchronize(ev_[1]));
@@ -491,6 +508,19 @@ class Runner {
     auto now = std::chrono::steady_clock::now();
     for (size_t i = 0; i < fin.size(); i++) {
       Job* j = fin[i];
+      // lists of one entry per state cannot overflow; list indices are 32-bit
+      const uint64_t cap_max = std::min<uint64_t>((uint64_t)g_->V * j->WT, 1ull << 31);
+      if (j->status == GST_QUEUE_OVERFLOW && (uint64_t)j->qd.cap < cap_max) {
+        // a frontier outgrew its list: run the query again with 4x the capacity
+        j->cap_req = std::min<uint64_t>(cap_max, (uint64_t)j->qd.cap * 4);
+        j->retries++;
+        Layout L = layout_for(g_, j->k, j->nd, j->members.size(), max_edges_dev_, j->cap_req);
+        j->bytes = L.total;
+        j->status = GST_OK;
+        j->edges.clear();
+        retry_.push_back(j);
+        continue;
+      }
       if (j->status == GST_OK && !j->edges.empty() && fin_off[i] != (size_t)-1)
         memcpy(j->edges.data(), estage + fin_off[i], j->edges.size() * 4);
       j->t_done = now;
@@ -502,6 +532,7 @@ class Runner {
   }
 
   gst_graph* g_;
+  std::deque<Job*> retry_;  // queries to run again with larger frontier lists
   cudaStream_t stream_ = nullptr;
   std::vector<Job*> slots_;
   uint32_t n_used_ = 0, nslots_hi_ = 0, max_slots_ = MAX_SLOTS - 1;
@@ -535,6 +566,7 @@ gst_status fill_result(Job* j, gst_result* r) {
   r->root = j->root;
   for (int i = 0; i < GST_NSTATS; i++) r->stats[i] = j->ctl.stat[i];
   r->stats[GST_STAT_TABLE_BYTES] = j->table_bytes;
+  r->stats[GST_STAT_RETRIES] = j->retries;
   r->latency_ms = std::chrono::duration<double, std::milli>(j->t_done - j->t_submit).count();
   gst_status st = j->status;
   if (st == GST_OK) {

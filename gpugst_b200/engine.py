@@ -29,7 +29,7 @@ STATUS_NAMES = {0: "ok", 1: "no solution", 2: "bad input", 3: "out of memory", 4
                 5: "cuda error", 6: "queue overflow", 7: "truncated", 8: "internal", 9: "busy",
                 10: "not found", 11: "scratch too small"}
 STAT_NAMES = ["expanded", "sssp_items", "arcs", "updates", "enqueued", "rounds", "merges", "table_bytes",
-              "sssp_arcs", "sssp_updates", "sssp_enqueued", "reserved"]
+              "sssp_arcs", "sssp_updates", "sssp_enqueued", "retries"]
 NSTATS = len(STAT_NAMES)
 KMAX = 8
 

@@ -47,7 +47,8 @@ typedef enum gst_status {
   GST_OOM = 3,              /* device memory for the state table not available */
   GST_DEVICE_TIMEOUT = 4,   /* a bounded device wait expired */
   GST_CUDA_ERROR = 5,       /* a CUDA runtime call failed */
-  GST_QUEUE_OVERFLOW = 6,   /* a frontier exceeded its capacity */
+  GST_QUEUE_OVERFLOW = 6,   /* a frontier exceeded its capacity: gst_query_noalloc only; the
+                               other entry points rerun the query with 4x larger lists */
   GST_TRUNCATED = 7,        /* tree has more edges than the caller's buffer */
   GST_INTERNAL = 8,         /* internal consistency check failed */
   GST_BUSY = 9,             /* serving: no free slot right now (submit again) */
@@ -71,7 +72,7 @@ enum {
   GST_STAT_SSSP_ARCS = 8,   /* arcs scanned by distance items */
   GST_STAT_SSSP_UPDATES = 9,  /* successful distance lowerings */
   GST_STAT_SSSP_ENQUEUED = 10, /* distance frontier insertions */
-  GST_STAT_RESERVED = 11,
+  GST_STAT_RETRIES = 11,    /* runs repeated with 4x larger frontier lists after GST_QUEUE_OVERFLOW */
   GST_NSTATS = 12
 };
 

@@ -88,21 +88,30 @@ def test_groups_set_rejects_bad_members(gst_lib):
 
 
 @pytest.mark.gpu
-def test_queue_overflow_is_reported(tmp_path):
-    """A frontier larger than GSTB_QUEUE_CAP returns GST_QUEUE_OVERFLOW instead
-    of writing out of bounds (run in a child process with a tiny capacity)."""
+def test_queue_overflow_is_retried_or_reported(tmp_path):
+    """A frontier larger than GSTB_QUEUE_CAP never writes out of bounds.  The
+    allocating entry points rerun the query with 4x larger lists (the
+    "retries" statistic counts the reruns); the allocation-free entry point,
+    whose scratch cannot grow, returns GST_QUEUE_OVERFLOW.  Run in a child
+    process with a tiny capacity."""
     code = r'''
 import sys, numpy as np
 sys.path.insert(0, %r)
 from gpugst_b200 import engine, gen
 g, gr = gen.small_instance(3000, 30000, 200, 20, seed=8)
 E = engine.Engine.from_instance(g, gr)
-r = E.query(np.array([0, 1, 2, 3], np.uint32))
-print("STATUS", r.status)
+q = np.array([0, 1, 2, 3], np.uint32)
+r = E.query(q)
+print("STATUS", r.status, "RETRIES", r.stats["retries"])
+r2 = E.query_noalloc(q)
+print("NOALLOC", r2.status)
 ''' % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))),)
     env = dict(os.environ, GSTB_QUEUE_CAP="1")
     out = subprocess.run(["python", "-c", code], capture_output=True, text=True, env=env, timeout=300)
-    assert "STATUS 6" in out.stdout, out.stdout + out.stderr
+    lines = dict(l.split(" ", 1) for l in out.stdout.splitlines() if l)
+    assert lines.get("STATUS", "").startswith("0 RETRIES "), out.stdout + out.stderr
+    assert int(lines["STATUS"].split()[-1]) > 0, out.stdout
+    assert lines.get("NOALLOC") == "6", out.stdout + out.stderr
 
 
 @pytest.mark.gpu

@@ -135,6 +135,29 @@ def test_batch_alone_vs_mixed(gst_lib, c1):
         assert a.cost == m.cost
 
 
+def test_queue_overflow_retry(gst_lib, oracle_mod, c1, monkeypatch):
+    """Frontier lists far too small for the query: the engine reruns each
+    overflowed query with 4x larger lists and still returns the optimum."""
+    eng, O = gst_lib, oracle_mod
+    g, gr, qs = c1
+    monkeypatch.setenv("GSTB_QUEUE_CAP", "1024")
+    E = _engine(eng, g, gr)
+    queries = list(qs[3][:8])
+    Ds = [-1] * 4 + [3] * 4
+    res = E.query_batch(queries, Ds)
+    one = E.query(queries[0])
+    E.close()
+    assert sum(r.stats["retries"] for r in res) > 0
+    for q, D, r in zip(queries, Ds, res):
+        want = O.prunedpp(g, gr, q, 0) if D < 0 else O.hop(g, gr, q, D)
+        if want.status != 0:
+            assert r.status == eng.GST_NO_SOLUTION, (D, r.status)
+            continue
+        assert r.status == eng.GST_OK and r.cost == want.cost, (D, want.cost, r.status, r.cost)
+        assert not O.validate(g, gr, q, D, r.cost, r.root, r.edges)
+    assert one.status == eng.GST_OK and one.cost == res[0].cost
+
+
 def test_edge_cases(gst_lib, oracle_mod):
     eng, O = gst_lib, oracle_mod
     # path 0-1-2-3 plus isolated vertex 4
