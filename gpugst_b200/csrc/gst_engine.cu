@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -109,6 +110,128 @@ struct Job {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// Device workspace arena of one Runner: chunks from cudaMalloc, carved by
+// best fit with coalescing.  Admission never waits on the driver's allocator
+// (a stream-ordered pool that had to grow stalled the serving loop for up to
+// half a second).  A block is reusable as soon as it is freed: every kernel,
+// copy and memset that touches a workspace runs on the Runner's one stream, so
+// work enqueued for the next owner is ordered after the last use.
+class Arena {
+ public:
+  ~Arena() { release(); }
+
+  void* alloc(size_t n) {
+    n = align_up(std::max<size_t>(n, 1), 256);
+    auto it = by_size_.lower_bound(n);
+    if (it == by_size_.end()) {
+      if (!grow(n)) return nullptr;
+      it = by_size_.lower_bound(n);
+      if (it == by_size_.end()) return nullptr;
+    }
+    char* p = it->second;
+    const size_t sz = it->first;
+    by_size_.erase(it);
+    free_.erase(p);
+    free_total_ -= sz;
+    if (sz > n) insert_free(p + n, sz - n);
+    used_[p] = n;
+    in_use_ += n;
+    return p;
+  }
+
+  void free(void* vp) {
+    char* p = static_cast<char*>(vp);
+    auto u = used_.find(p);
+    if (u == used_.end()) return;
+    size_t n = u->second;
+    used_.erase(u);
+    in_use_ -= n;
+    const char* base = chunk_base(p);
+    // merge with the free neighbours inside the same chunk
+    auto nx = free_.find(p + n);
+    if (nx != free_.end() && chunk_base(nx->first) == base) {
+      n += nx->second;
+      erase_free(nx->first, nx->second);
+    }
+    auto pv = free_.lower_bound(p);
+    if (pv != free_.begin()) {
+      --pv;
+      if (pv->first + pv->second == p && chunk_base(pv->first) == base) {
+        char* q = pv->first;
+        n += pv->second;
+        erase_free(q, pv->second);
+        p = q;
+      }
+    }
+    insert_free(p, n);
+  }
+
+  // Make at least n bytes free with one allocation instead of several growth
+  // steps later (called before a batch or when a serving loop opens).
+  bool reserve(size_t n) {
+    if (free_total_ >= n) return true;
+    return grow(align_up(n - free_total_, 256), true);
+  }
+
+  void release() {
+    for (auto& c : chunks_) cudaFree(c.first);
+    chunks_.clear();
+    free_.clear();
+    by_size_.clear();
+    used_.clear();
+    held_ = in_use_ = free_total_ = 0;
+  }
+
+
+ private:
+  bool grow(size_t n, bool exact = false) {
+    // chunks double from 64 MB up to GSTB_ARENA_MB (default 1 GB)
+    const size_t step = (size_t)env_u32("GSTB_ARENA_MB", 1024) << 20;
+    void* p = nullptr;
+    size_t sz = exact ? n : std::max(n, std::min(step, std::max<size_t>(held_, 64ull << 20)));
+    if (cudaMalloc(&p, sz) != cudaSuccess) {
+      cudaGetLastError();
+      sz = n;
+      if (cudaMalloc(&p, sz) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+      }
+    }
+    chunks_[static_cast<char*>(p)] = sz;
+    held_ += sz;
+    insert_free(static_cast<char*>(p), sz);
+    return true;
+  }
+
+  const char* chunk_base(const char* p) const {
+    auto it = chunks_.upper_bound(const_cast<char*>(p));
+    return it == chunks_.begin() ? nullptr : std::prev(it)->first;
+  }
+
+  void insert_free(char* p, size_t n) {
+    free_[p] = n;
+    by_size_.emplace(n, p);
+    free_total_ += n;
+  }
+
+  void erase_free(char* p, size_t n) {
+    free_.erase(p);
+    free_total_ -= n;
+    auto r = by_size_.equal_range(n);
+    for (auto it = r.first; it != r.second; ++it)
+      if (it->second == p) {
+        by_size_.erase(it);
+        break;
+      }
+  }
+
+  std::map<char*, size_t> chunks_;        // base -> size
+  std::map<char*, size_t> free_;          // free block -> size
+  std::multimap<size_t, char*> by_size_;  // size -> free block
+  std::unordered_map<char*, size_t> used_;
+  size_t held_ = 0, in_use_ = 0, free_total_ = 0;
+};
+
 // Workspace layout of one query (see gst_device.cuh).
 struct Layout {
   size_t table, dist, dflag, sflag, qbuf, tour, lbt, members, edges, total;
@@ -122,7 +245,10 @@ Layout layout_for(const gst_graph* g, int k, int nd, size_t n_members, uint32_t 
   uint64_t WT = (uint64_t)(1u << k) * nd;
   uint64_t states = (uint64_t)g->V * WT;
   uint64_t caplim = env_u32("GSTB_QUEUE_CAP", 1u << 25);
-  uint64_t cap = std::max<uint64_t>(std::min<uint64_t>(states, caplim), std::min<uint64_t>((uint64_t)g->V * k, caplim));
+  // distance lists hold each vertex at most once per list (cap >= V never
+  // overflows there); DP lists start at a quarter of the states and grow by
+  // rerunning the query if a frontier outgrows them
+  uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(states / 4, (uint64_t)g->V + 1024), caplim);
   if (cap_req) cap = cap_req;
   cap = std::max<uint64_t>(cap, 1024);
   L.cap = (uint32_t)cap;
@@ -159,16 +285,13 @@ class Runner {
     CK(cudaEventCreateWithFlags(&ev_fin_, cudaEventDisableTiming));
     for (auto& hh : ev_prof_)
       for (auto& e : hh) CK(cudaEventCreate(&e));
-    cudaMemPool_t pool;
-    CK(cudaDeviceGetDefaultMemPool(&pool, g_->device));
-    uint64_t thr = ~0ull;
-    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
     delta_sssp_ = std::max(1u, env_u32("GSTB_DELTA_SSSP", 16));
     delta_dp_ = std::max(1u, env_u32("GSTB_DELTA_DP", 4));
     cap_num_ = std::max(1u, env_u32("GSTB_SSSP_CAP_NUM", 1));
     cap_den_ = std::max(1u, env_u32("GSTB_SSSP_CAP_DEN", 2));
     max_edges_dev_ = env_u32("GSTB_MAX_TREE_EDGES", 1u << 16);
     rounds_per_sync_ = std::min(64u, std::max(1u, env_u32("GSTB_ROUNDS_PER_SYNC", 4)));
+    trace_ms_ = (double)env_u32("GSTB_TRACE_MS", 0);  // report host iterations slower than this
     max_slots_ = std::min<uint32_t>(MAX_SLOTS - 1, std::max(1u, env_u32("GSTB_MAX_SLOTS", MAX_SLOTS - 1)));
     CK(cudaMalloc(&d_qd_, MAX_SLOTS * sizeof(QDev)));
     CK(cudaMalloc(&d_ctl_, MAX_SLOTS * sizeof(QCtl)));
@@ -234,6 +357,8 @@ class Runner {
     for (auto& hh : ev_prof_)
       for (auto& e : hh)
         if (e) cudaEventDestroy(e);
+    if (stream_) cudaStreamSynchronize(stream_);
+    arena_.release();
     if (stream_) cudaStreamDestroy(stream_);
     d_qd_ = nullptr;
     d_ctl_ = nullptr;
@@ -273,6 +398,7 @@ class Runner {
   }
 
   bool has_free_slot() const { return n_used_ < max_slots_; }
+  bool reserve(size_t bytes) { return arena_.reserve(bytes); }
   size_t live() const { return n_used_; }
 
   // Allocate the workspace, initialise it and install the job in a free
@@ -282,11 +408,8 @@ class Runner {
     const size_t need = align_up(sizeof(QDev), 64) + align_up(sizeof(QCtl), 64) + align_up(j->members.size() * 4, 64);
     const int sh = (int)(next_block_ & 1);  // staging half of the block this job starts in
     if (stage_off_[sh] + need > stage_cap_ / 2) return false;  // staging full until that block has run
-    void* p = nullptr;
-    if (cudaMallocAsync(&p, j->bytes, stream_) != cudaSuccess) {
-      cudaGetLastError();
-      return false;
-    }
+    void* p = arena_.alloc(j->bytes);
+    if (p == nullptr) return false;
     int slot = -1;
     for (uint32_t s = 0; s < max_slots_; s++)
       if (!slots_[s]) {
@@ -356,7 +479,7 @@ class Runner {
   }
 
   void free_job(Job* j) {
-    if (j->mem) cudaFreeAsync(j->mem, stream_);
+    if (j->mem) arena_.free(j->mem);
     j->mem = nullptr;
   }
 
@@ -377,7 +500,11 @@ class Runner {
     std::vector<Job*> fin;  // retired jobs whose tree copies are in flight
     std::vector<size_t> fin_off;
     int fin_half = 0;
+    using clk = std::chrono::steady_clock;
+    auto ms_since = [](clk::time_point a) { return std::chrono::duration<double, std::milli>(clk::now() - a).count(); };
     for (;;) {
+      const clk::time_point t_it = clk::now();
+      double t_admit = 0, t_launch = 0, t_fin = 0, t_blk = 0;
       // queries retried with larger frontier lists go first
       while (!retry_.empty() && has_free_slot()) {
         Job* j = retry_.front();
@@ -393,25 +520,37 @@ class Runner {
         retry_.pop_front();
       }
       admit_more();
+      if (trace_ms_ > 0) t_admit = ms_since(t_it);
       int64_t launched = -1;
       if (n_used_ > 0) {
         gst_status st = launch_block(rounds_per_sync_);
         if (st != GST_OK) return st;
         launched = next_block_++;
       }
+      if (trace_ms_ > 0) t_launch = ms_since(t_it);
       if (!fin.empty()) {
         CK(cudaEventSynchronize(ev_fin_));
         finalize(fin, fin_off, fin_half, on_done);
       }
+      if (trace_ms_ > 0) t_fin = ms_since(t_it);
       if (inflight >= 0) {
         const int h = (int)(inflight & 1);
         CK(cudaEventSynchronize(ev_blk_[h]));
+        if (trace_ms_ > 0) t_blk = ms_since(t_it);
         stage_off_[h] = 0;  // admissions staged for this block have been copied
         if (g_->profile) accumulate_profile(h);
         gst_status st = detect_done(inflight, fin, fin_off);
         if (st != GST_OK) return st;
         fin_half = h;
         if (!fin.empty()) CK(cudaEventRecord(ev_fin_, stream_));
+      }
+      if (trace_ms_ > 0) {
+        const double t_all = ms_since(t_it);
+        if (t_all >= trace_ms_)
+          fprintf(stderr,
+                  "gstb: slow host iteration %.2f ms (admit %.2f, launch %.2f, finalize %.2f, block wait %.2f; "
+                  "%u queries in slots)\n",
+                  t_all, t_admit, t_launch - t_admit, t_fin - t_launch, t_blk > 0 ? t_blk - t_fin : 0.0, n_used_);
       }
       inflight = launched;
       if (inflight < 0 && n_used_ == 0 && fin.empty() && retry_.empty()) break;
@@ -532,6 +671,7 @@ class Runner {
   }
 
   gst_graph* g_;
+  Arena arena_;
   std::deque<Job*> retry_;  // queries to run again with larger frontier lists
   cudaStream_t stream_ = nullptr;
   std::vector<Job*> slots_;
@@ -557,6 +697,7 @@ class Runner {
   cudaEvent_t ev_[2] = {};
   unsigned light_grid_ = 148 * 4, heavy_grid_ = 148 * 2;
   double last_call_ms_ = 0;
+  double trace_ms_ = 0;
 };
 
 // Copy a finished job into a caller result.
@@ -796,6 +937,17 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
     pending.push_back(&j);
   }
   const size_t maxc = max_concurrent > 0 ? (size_t)max_concurrent : (size_t)1 << 20;
+  {
+    // workspace for the first wave of the batch in one arena allocation
+    size_t need = 0, cnt = 0;
+    for (Job* j : pending) {
+      if (cnt++ >= std::min<size_t>(maxc, MAX_SLOTS - 1)) break;
+      need += align_up(j->bytes, 256);
+    }
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) need = std::min(need, (size_t)(fr * 0.8));
+    R.reserve(need);  // best effort: admission still grows the arena or waits
+  }
   gst_status rs = R.run(
       [&]() {
         while (!pending.empty() && R.live() < maxc && R.has_free_slot()) {
@@ -911,6 +1063,8 @@ gst_status gst_serve_open(gst_graph* g, uint64_t hbm_budget_bytes, int max_infli
     hbm_budget_bytes = (uint64_t)(fr * 0.8);
   }
   S->budget = hbm_budget_bytes;
+  // grow the workspace arena once now rather than while requests wait
+  S->runner->reserve(std::min<uint64_t>(hbm_budget_bytes, (uint64_t)env_u32("GSTB_SERVE_RESERVE_MB", 4096) << 20));
   S->max_inflight = max_inflight > 0 ? (size_t)max_inflight : (size_t)(MAX_SLOTS - 1);
   S->th = std::thread(serve_loop, S);
   *out = S;

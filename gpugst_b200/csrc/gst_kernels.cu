@@ -6,8 +6,9 @@
 //              (distance rounds -> tour tables -> DP seed -> DP rounds ->
 //              extraction) and writes the round's work description;
 //   k_light    warp tasks: near-far splits, seeds, tour tables, extraction and
-//              distance items (8 lanes per (vertex, group) item: multi-source
-//              relax, replacing dis0_init_1, DPQ.cu:241-271);
+//              distance items (a vertex with its pending groups; the arcs of
+//              a task's items are relaxed as one flat list by the whole warp:
+//              multi-source relax, replacing dis0_init_1, DPQ.cu:241-271);
 //   k_heavy    warp per DP state:
 //                   DP item       : best update from complement / one-label
 //                                   completion, lower-bound prune, grow along
@@ -388,240 +389,369 @@ __device__ __forceinline__ uint32_t find_slot_s(const uint32_t* pre, int nslots,
 }
 
 // ---------------------------------------------------------------------------
-// Distance items: one warp task = 4 items, 8 lanes each.  The weight-sorted
-// adjacency usually leaves only a few arcs under the limit, so a full warp
-// per item would idle most lanes.  Counters are kept per lane group and
-// flushed when the group moves to another query (and at kernel end).
+// Distance items.  A warp task holds up to SSSP_W items (a vertex with the
+// mask of its pending groups).  Lanes 0..SSSP_W-1 read the items' headers in
+// parallel; then the arcs of all items of the task are relaxed as one flat
+// list, 32 x SSSP_U arcs per step.  Each lane keeps SSSP_U independent
+// chains (arc -> distance row -> pending flag) in flight, and uneven degrees
+// are spread over all 32 lanes instead of one lane group per item.
 // ---------------------------------------------------------------------------
-struct SsspCounters {
+constexpr int SSSP_W = 4;            // items per warp task (k_control's per-task count)
+constexpr int SSSP_U = 4;            // arcs per lane per step
+constexpr uint32_t HUB_LOCAL = 32;   // arcs of a hub item its own task relaxes
+
+struct alignas(16) RelaxHdr {
+  uint32_t d[KMAX];  // group distances at the item's vertex
+  uint32_t rm;       // groups to relax from it
+  uint32_t lim;      // largest arc weight that can still lower a distance
+  uint32_t a0;       // first arc to relax
+  uint32_t pad;
+};
+
+struct RelaxCnt {
+  uint32_t arcs = 0, upd = 0, enq = 0;
+};
+
+// Per-warp statistics of one query, flushed when the warp moves to another
+// query and at kernel end (held by lane 0).
+struct SsspAcc {
   QCtl* cur = nullptr;
   uint32_t items = 0, arcs = 0, upd = 0, enq = 0;
 };
 
-__device__ __forceinline__ void sssp_flush(SsspCounters& sc, uint32_t sl) {
-  const unsigned FULL = 0xFFFFFFFFu;
-  uint32_t a = sc.arcs, u = sc.upd, e = sc.enq;
+__device__ __forceinline__ void sssp_acc_flush(SsspAcc& a) {
+  if (a.cur) {
+    if (a.items) atomicAdd(&a.cur->stat[ST_SSSP], (unsigned long long)a.items);
+    if (a.arcs) atomicAdd(&a.cur->stat[ST_SSSP_ARCS], (unsigned long long)a.arcs);
+    if (a.upd) atomicAdd(&a.cur->stat[ST_SSSP_UPDATES], (unsigned long long)a.upd);
+    if (a.enq) atomicAdd(&a.cur->stat[ST_SSSP_ENQ], (unsigned long long)a.enq);
+  }
+  a.items = a.arcs = a.upd = a.enq = 0;
+}
+
+__device__ __forceinline__ uint32_t warp_sum(uint32_t x) {
 #pragma unroll
-  for (int o = 4; o > 0; o >>= 1) {
-    a += __shfl_xor_sync(FULL, a, o);
-    u += __shfl_xor_sync(FULL, u, o);
-    e += __shfl_xor_sync(FULL, e, o);
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, o);
+  return x;
+}
+
+__device__ __forceinline__ uint32_t sel8(const uint4& a, const uint4& b, uint32_t i) {
+  const uint4& h = i < 4u ? a : b;
+  const uint32_t j = i & 3u;
+  return j == 0u ? h.x : (j == 1u ? h.y : (j == 2u ? h.z : h.w));
+}
+
+// Relax the arcs [h[i].a0, h[i].a0 + n_i) of W items of query q, where
+// ends[i] = n_0 + ... + n_i (warp-uniform).  Every lane of the warp calls it.
+// A lowered distance is written with a fire-and-forget atomicMin after a
+// pre-check; the pending-groups flag of the target gates its list entry
+// (parity-split flags, so no update is lost); appends are aggregated over
+// the whole warp.
+template <int W>
+__device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __restrict__ h, const uint32_t (&ends)[W],
+                                           uint32_t capb, const GraphDev& g, uint32_t lane, RelaxCnt& cnt) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  const uint32_t total = ends[W - 1];
+  const uint32_t V = q.nv, thi = q.theta_hi;
+  uint32_t* __restrict__ dist = q.dist;
+  uint32_t* pnext = q.sflag + (size_t)(q.par ^ 1u) * V;
+  uint32_t* pfar = q.sflag + (size_t)2 * V;
+  for (uint32_t base = 0; base < total; base += 32u * SSSP_U) {
+    uint2 arc[SSSP_U];
+    uint32_t itm[SSSP_U];
+    bool ok[SSSP_U];
+#pragma unroll
+    for (int u = 0; u < SSSP_U; u++) {
+      const uint32_t f = base + (uint32_t)u * 32u + lane;
+      uint32_t i = 0, start = 0;
+#pragma unroll
+      for (int j = 0; j < W - 1; j++)
+        if (f >= ends[j]) {
+          i = (uint32_t)j + 1u;
+          start = ends[j];
+        }
+      itm[u] = i;
+      ok[u] = f < total;
+      arc[u] = ok[u] ? __ldg(g.adj + h[i].a0 + (f - start)) : make_uint2(0u, 0u);
+    }
+    uint4 ra[SSSP_U], rb[SSSP_U];
+#pragma unroll
+    for (int u = 0; u < SSSP_U; u++) {
+      ok[u] = ok[u] && arc[u].y <= h[itm[u]].lim;
+      if (ok[u]) {
+        const uint4* row = reinterpret_cast<const uint4*>(dist + (size_t)arc[u].x * 8);
+        ra[u] = __ldcg(row);
+        rb[u] = __ldcg(row + 1);
+      } else {
+        ra[u] = rb[u] = make_uint4(0u, 0u, 0u, 0u);
+      }
+    }
+    uint32_t nn[SSSP_U], nf[SSSP_U];
+#pragma unroll
+    for (int u = 0; u < SSSP_U; u++) {
+      nn[u] = nf[u] = 0u;
+      if (ok[u]) {
+        cnt.arcs++;
+        const RelaxHdr& hh = h[itm[u]];
+        const uint32_t rm = hh.rm;
+        const uint32_t du[8] = {ra[u].x, ra[u].y, ra[u].z, ra[u].w, rb[u].x, rb[u].y, rb[u].z, rb[u].w};
+#pragma unroll
+        for (int t = 0; t < KMAX; t++) {
+          if ((rm >> t) & 1u) {
+            const uint32_t dt = hh.d[t];
+            const uint32_t nd = dt + arc[u].y;
+            if (nd >= dt && nd <= capb && nd < du[t]) {
+              atomicMin(dist + (size_t)arc[u].x * 8 + t, nd);  // result not needed
+              if (nd < thi)
+                nn[u] |= 1u << t;
+              else
+                nf[u] |= 1u << t;
+              cnt.upd++;
+            }
+          }
+        }
+      }
+    }
+    // all flag updates of the step are issued before any result is used
+    uint32_t oN[SSSP_U], oF[SSSP_U];
+#pragma unroll
+    for (int u = 0; u < SSSP_U; u++) {
+      oN[u] = nn[u] ? atomicOr(pnext + arc[u].x, nn[u]) : 1u;
+      oF[u] = nf[u] ? atomicOr(pfar + arc[u].x, nf[u]) : 1u;
+    }
+    uint32_t cN = 0, cF = 0;
+#pragma unroll
+    for (int u = 0; u < SSSP_U; u++) {
+      cN += oN[u] == 0u;
+      cF += oF[u] == 0u;
+    }
+    if (!__any_sync(FULL, (cN | cF) != 0u)) continue;
+    // one list reservation per warp and list
+    uint32_t xN = cN, xF = cF;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t yN = __shfl_up_sync(FULL, xN, o), yF = __shfl_up_sync(FULL, xF, o);
+      if (lane >= (uint32_t)o) {
+        xN += yN;
+        xF += yF;
+      }
+    }
+    const uint32_t totN = __shfl_sync(FULL, xN, 31), totF = __shfl_sync(FULL, xF, 31);
+    uint32_t bN = 0, bF = 0;
+    if (lane == 0) {
+      if (totN) bN = atomicAdd(&q.ctl->n_near, totN);
+      if (totF) bF = atomicAdd(&q.ctl->n_far, totF);
+    }
+    uint32_t pN = __shfl_sync(FULL, bN, 0) + xN - cN, pF = __shfl_sync(FULL, bF, 0) + xF - cF;
+    uint32_t* outN = q.qbuf[q.out_idx];
+    uint32_t* outF = q.qbuf[q.far_idx];
+    bool ovf = false;
+#pragma unroll
+    for (int u = 0; u < SSSP_U; u++) {
+      if (oN[u] == 0u) {
+        if (pN < q.cap)
+          outN[pN] = arc[u].x;
+        else
+          ovf = true;
+        pN++;
+      }
+      if (oF[u] == 0u) {
+        if (pF < q.cap)
+          outF[pF] = arc[u].x;
+        else
+          ovf = true;
+        pF++;
+      }
+    }
+    if (ovf) atomicExch(&q.ctl->overflow, 1u);
+    cnt.enq += cN + cF;
   }
-  if (sc.cur && sl == 0) {
-    if (sc.items) atomicAdd(&sc.cur->stat[ST_SSSP], (unsigned long long)sc.items);
-    if (a) atomicAdd(&sc.cur->stat[ST_SSSP_ARCS], (unsigned long long)a);
-    if (u) atomicAdd(&sc.cur->stat[ST_SSSP_UPDATES], (unsigned long long)u);
-    if (e) atomicAdd(&sc.cur->stat[ST_SSSP_ENQ], (unsigned long long)e);
+}
+
+__device__ __forceinline__ void relax_cnt_flush(QCtl* c, RelaxCnt cnt, uint32_t items, uint32_t lane) {
+  const uint32_t a = warp_sum(cnt.arcs), u = warp_sum(cnt.upd), e = warp_sum(cnt.enq);
+  if (lane == 0) {
+    if (items) atomicAdd(&c->stat[ST_SSSP], (unsigned long long)items);
+    if (a) atomicAdd(&c->stat[ST_SSSP_ARCS], (unsigned long long)a);
+    if (u) atomicAdd(&c->stat[ST_SSSP_UPDATES], (unsigned long long)u);
+    if (e) atomicAdd(&c->stat[ST_SSSP_ENQ], (unsigned long long)e);
   }
-  sc.items = sc.arcs = sc.upd = sc.enq = 0;
 }
 
 __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restrict__ pre, int nslots,
-                          uint32_t total, uint32_t task, const GraphDev& g, uint32_t lane, SsspCounters& sc,
-                          RoundDesc* __restrict__ rd) {
+                          uint32_t total, uint32_t task, const GraphDev& g, uint32_t lane, SsspAcc& acc,
+                          RoundDesc* __restrict__ rd, RelaxHdr* __restrict__ sh) {
   const unsigned FULL = 0xFFFFFFFFu;
-  const uint32_t sub = lane >> 3, sl = lane & 7u, gbase = lane & ~7u;
-  const uint32_t it = task * 4u + sub;
-  const bool valid = it < total;
-  const uint32_t slot = valid ? find_slot_s(pre, nslots, it) : 0u;
-  const QDev& q = qd[slot];
-  // flush the group's counters when it changes query (group-uniform decision)
-  bool change = valid && q.ctl != sc.cur;
-  if (__any_sync(FULL, change)) {
-    unsigned cm = __ballot_sync(FULL, change);
-    bool mine = (cm >> gbase) & 1u;
-    uint32_t a = sc.arcs, u = sc.upd, e = sc.enq;
-#pragma unroll
-    for (int o = 4; o > 0; o >>= 1) {
-      a += __shfl_xor_sync(FULL, a, o);
-      u += __shfl_xor_sync(FULL, u, o);
-      e += __shfl_xor_sync(FULL, e, o);
+  const uint32_t it = task * (uint32_t)SSSP_W + lane;
+  const bool valid = lane < (uint32_t)SSSP_W && it < total;
+  const uint32_t slot = valid ? find_slot_s(pre, nslots, it) : 0xFFFFFFFFu;
+  uint32_t n = 0, capb = INF32;
+  bool active = false;
+  if (valid) {
+    const QDev& q = qd[slot];
+    const uint32_t V = q.nv;
+    const int k = q.k;
+    const uint32_t v = q.qbuf[q.in_idx][it - pre[slot]];
+    // the header's loads depend on v only, so they are all in flight at once
+    const uint32_t m = atomicExch(&q.sflag[(size_t)q.par * V + v], 0u);
+    const uint4* drow = reinterpret_cast<const uint4*>(q.dist + (size_t)v * 8);
+    const uint4 da = __ldcg(drow), db = __ldcg(drow + 1);
+    uint32_t best = ld_cg(&q.ctl->best);
+    const uint32_t b0 = __ldg(g.beg + v), b1 = __ldg(g.beg + v + 1);
+    uint4 wa = make_uint4(b1, b1, b1, b1), wb = wa;
+    if (g.wcut != nullptr) {
+      const uint4* wr = reinterpret_cast<const uint4*>(g.wcut + (size_t)v * 8);
+      wa = __ldg(wr);
+      wb = __ldg(wr + 1);
     }
-    if (mine) {
-      if (sc.cur && sl == 0) {
-        if (sc.items) atomicAdd(&sc.cur->stat[ST_SSSP], (unsigned long long)sc.items);
-        if (a) atomicAdd(&sc.cur->stat[ST_SSSP_ARCS], (unsigned long long)a);
-        if (u) atomicAdd(&sc.cur->stat[ST_SSSP_UPDATES], (unsigned long long)u);
-        if (e) atomicAdd(&sc.cur->stat[ST_SSSP_ENQ], (unsigned long long)e);
-      }
-      sc.items = sc.arcs = sc.upd = sc.enq = 0;
-      sc.cur = q.ctl;
-    }
-  }
-  const uint32_t V = q.nv;
-  const uint32_t v = valid ? q.qbuf[q.in_idx][it - pre[slot]] : 0u;
-  // take the groups whose distance at v changed into this window
-  uint32_t m = 0;
-  if (valid && sl == 0) m = atomicExch(&q.sflag[(size_t)q.par * V + v], 0u);
-  m = __shfl_sync(FULL, m, gbase);
-  const int k = valid ? q.k : 0;
-  // lane sl holds d_sl(v)
-  const uint32_t dj = (valid && sl < (uint32_t)k) ? ld_cg(q.dist + (size_t)v * 8 + sl) : INF32;
-  uint32_t best = __shfl_sync(FULL, valid ? ld_cg(&q.ctl->best) : 0u, gbase);
-  // star bound at v (unbounded queries only): v joined to every group by
-  // shortest paths, a feasible tree (one-label completion, CPUNONHOP.h:684-699)
-  {
-    bool lanev = valid && q.D < 0 && sl < (uint32_t)k;
-    unsigned bad = __ballot_sync(FULL, lanev && dj == INF32);
-    unsigned long long sum = lanev ? dj : 0u;
-    sum += __shfl_xor_sync(FULL, sum, 4);
-    sum += __shfl_xor_sync(FULL, sum, 2);
-    sum += __shfl_xor_sync(FULL, sum, 1);
-    if (valid && q.D < 0 && sl == 0 && ((bad >> gbase) & 0xFFu) == 0 && sum < best)
-      atomicMin(&q.ctl->best, (uint32_t)sum);
-  }
-  best = __shfl_sync(FULL, valid ? ld_cg(&q.ctl->best) : 0u, gbase);
-  // distances beyond cap(best) cannot lower a bound below best: skip them
-  const uint32_t capb = valid ? (uint32_t)((unsigned long long)best * q.cap_num / q.cap_den) : 0u;
-  const bool rl = valid && sl < (uint32_t)k && ((m >> sl) & 1u) && dj <= capb;
-  const uint32_t rm = (__ballot_sync(FULL, rl) >> gbase) & 0xFFu;  // groups to relax
-  uint32_t dmin = rl ? dj : INF32;
-  dmin = min(dmin, __shfl_xor_sync(FULL, dmin, 4));
-  dmin = min(dmin, __shfl_xor_sync(FULL, dmin, 2));
-  dmin = min(dmin, __shfl_xor_sync(FULL, dmin, 1));
-  uint32_t d[KMAX];
+    const uint32_t d[8] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z, db.w};
+    // star bound at v (unbounded queries only): v joined to every group by
+    // shortest paths is a feasible tree (one-label completion, CPUNONHOP.h:684-699)
+    if (q.D < 0) {
+      unsigned long long sum = 0;
+      bool fin = true;
 #pragma unroll
-  for (int t = 0; t < KMAX; t++) d[t] = __shfl_sync(FULL, dj, gbase + t);
-  const bool active = rm != 0;
-  const uint32_t lim = active ? capb - dmin : 0u;
-  const uint32_t a0 = active ? __ldg(g.beg + v) : 0u;
-  const uint32_t a1 = active ? arcs_upto(g, v, __ldg(g.beg + v + 1), lim) : 0u;
-  if (active && sl == 0) sc.items++;
-  const uint32_t thi = valid ? q.theta_hi : 0u;
-  uint32_t* pnext = valid ? q.sflag + (size_t)(q.par ^ 1u) * V : nullptr;
-  uint32_t* pfar = valid ? q.sflag + (size_t)2 * V : nullptr;
-  bool done = !active;
-  for (uint32_t off = 0;; off += 8) {
-    bool more = !done && a0 + off < a1;
-    if (!__any_sync(FULL, more)) break;
-    uint32_t a = a0 + off + sl;
-    bool in = more && a < a1;
-    uint2 arc = in ? __ldg(g.adj + a) : make_uint2(0, 0xFFFFFFFFu);
-    bool over = in && arc.y > lim;
-    bool takeN = false, takeF = false;
-    if (in && !over) {
-      sc.arcs++;
-      const uint32_t u = arc.x;
-      const uint4* row = reinterpret_cast<const uint4*>(q.dist + (size_t)u * 8);
-      uint4 ra = __ldcg(row), rb = __ldcg(row + 1);
-      uint32_t du[8] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
-      uint32_t nn = 0, nf = 0;
-#pragma unroll
-      for (int t = 0; t < KMAX; t++) {
-        if ((rm >> t) & 1u) {
-          uint32_t nd = d[t] + arc.y;
-          if (nd <= capb && nd < du[t]) {
-            atomicMin(q.dist + (size_t)u * 8 + t, nd);  // result not needed
-            if (nd < thi)
-              nn |= 1u << t;
-            else
-              nf |= 1u << t;
-            sc.upd++;
-          }
+      for (int t = 0; t < KMAX; t++)
+        if (t < k) {
+          fin = fin && d[t] != INF32;
+          sum += d[t];
         }
+      if (fin && sum < best) {
+        atomicMin(&q.ctl->best, (uint32_t)sum);
+        best = (uint32_t)sum;
       }
-      if (nn) takeN = atomicOr(pnext + u, nn) == 0u;
-      if (nf) takeF = atomicOr(pfar + u, nf) == 0u;
     }
-    append_multi(takeN, arc.x, true, q, slot, lane, sc.enq);
-    append_multi(takeF, arc.x, false, q, slot, lane, sc.enq);
-    unsigned stop = __ballot_sync(FULL, over || (more && a + 1 >= a1));
-    if ((stop >> gbase) & 0xFFu) done = true;  // sorted by weight: the rest is heavier
-    if (off == 0) {
-      // hub: many arcs left under the limit -> hand them to k_heavy in chunks
-      // of HUB_CHUNK arcs, one warp each, instead of 8 lanes walking them all
-      bool hub = !done && a1 - a0 >= rd->hub_min_deg && rd->hub_on;
-      uint32_t cut = 0, nch = 0, base = 0;
-      if (hub && sl == 0) {
-        cut = a1;  // already cut to the weight bucket of the limit
-        nch = (cut - (a0 + 8) + HUB_CHUNK - 1) / HUB_CHUNK;
-        if (rd->big == nullptr || cut - (a0 + 8) < rd->hub_min_rest) {
-          nch = 0xFFFFFFFFu;  // chunking disabled: keep walking here
-        } else if (nch > 0) {
-          base = atomicAdd(&rd->n_big, nch);
-          if (base + nch <= rd->big_cap) {
-            for (uint32_t c = 0; c < nch; c++) {
-              uint32_t st = a0 + 8 + c * HUB_CHUNK;
-              rd->big[base + c] = make_uint4(slot | (rm << 16), v, st, min(st + HUB_CHUNK, cut));
-            }
-          } else {
-            nch = 0xFFFFFFFFu;  // no room: keep walking here
-          }
-        }
+    // distances beyond cap(best) cannot lower a bound below best: skip them
+    capb = (uint32_t)((unsigned long long)best * q.cap_num / q.cap_den);
+    uint32_t rm = 0, dmin = INF32;
+#pragma unroll
+    for (int t = 0; t < KMAX; t++)
+      if (t < k && ((m >> t) & 1u) && d[t] <= capb) {
+        rm |= 1u << t;
+        dmin = min(dmin, d[t]);
       }
-      nch = __shfl_sync(FULL, nch, gbase);
-      if (hub && nch != 0xFFFFFFFFu) done = true;
+    active = rm != 0;
+    uint32_t lim = 0;
+    if (active) {
+      lim = capb - dmin;
+      uint32_t a1 = b1;
+      if (g.wcut != nullptr && lim <= 128u) a1 = sel8(wa, wb, lim <= 1u ? 0u : 32u - __clz(lim - 1u));
+      n = a1 - b0;
+      // hub: hand all but the first HUB_LOCAL arcs to k_heavy in chunks of
+      // HUB_CHUNK arcs, one warp each
+      if (rd->hub_on && n >= rd->hub_min_deg && n - HUB_LOCAL >= rd->hub_min_rest) {
+        const uint32_t st0 = b0 + HUB_LOCAL;
+        const uint32_t nch = (a1 - st0 + HUB_CHUNK - 1u) / HUB_CHUNK;
+        const uint32_t cb = atomicAdd(&rd->n_big, nch);
+        const bool fits = cb + nch <= rd->big_cap;
+        // entries below the cap are always written (empty ranges when the
+        // whole run does not fit) so k_heavy never reads a stale entry
+        for (uint32_t c = 0; c < nch && cb + c < rd->big_cap; c++) {
+          const uint32_t s0 = st0 + c * HUB_CHUNK;
+          rd->big[cb + c] = fits ? make_uint4(slot | (rm << 16), v, s0, min(s0 + HUB_CHUNK, a1))
+                                 : make_uint4(slot, v, 0u, 0u);
+        }
+        if (fits) n = HUB_LOCAL;
+      }
+    }
+    RelaxHdr hd;
+#pragma unroll
+    for (int t = 0; t < KMAX; t++) hd.d[t] = d[t];
+    hd.rm = rm;
+    hd.lim = lim;
+    hd.a0 = b0;
+    hd.pad = 0;
+    sh[lane] = hd;
+  }
+  __syncwarp();
+  const uint32_t slot0 = __shfl_sync(FULL, slot, 0);
+  if (slot0 == 0xFFFFFFFFu) return;
+  const uint32_t n_items = __popc(__ballot_sync(FULL, active));
+  if (__all_sync(FULL, !valid || slot == slot0)) {
+    // one query: the items' arcs form one flat list
+    uint32_t x = n;
+#pragma unroll
+    for (int o = 1; o < SSSP_W; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, x, o);
+      if (lane >= (uint32_t)o) x += y;
+    }
+    uint32_t ends[SSSP_W];
+#pragma unroll
+    for (int j = 0; j < SSSP_W; j++) ends[j] = __shfl_sync(FULL, x, j);
+    uint32_t cb = capb;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cb = min(cb, __shfl_xor_sync(FULL, cb, o));
+    const QDev& q = qd[slot0];
+    RelaxCnt cnt;
+    if (ends[SSSP_W - 1]) relax_flat<SSSP_W>(q, sh, ends, cb, g, lane, cnt);
+    const uint32_t a = warp_sum(cnt.arcs), u = warp_sum(cnt.upd), e = warp_sum(cnt.enq);
+    if (lane == 0) {
+      if (acc.cur != q.ctl) {
+        sssp_acc_flush(acc);
+        acc.cur = q.ctl;
+      }
+      acc.items += n_items;
+      acc.arcs += a;
+      acc.upd += u;
+      acc.enq += e;
+    }
+  } else {
+    // the task straddles queries (at most one task per query boundary and
+    // round): relax item by item
+    for (int i = 0; i < SSSP_W; i++) {
+      const uint32_t si = __shfl_sync(FULL, slot, i), ni = __shfl_sync(FULL, n, i);
+      const uint32_t ci = __shfl_sync(FULL, capb, i);
+      const bool ai = __shfl_sync(FULL, active, i);
+      if (si == 0xFFFFFFFFu) continue;
+      const QDev& q = qd[si];
+      RelaxCnt cnt;
+      const uint32_t e1[1] = {ni};
+      if (ni) relax_flat<1>(q, sh + i, e1, ci, g, lane, cnt);
+      relax_cnt_flush(q.ctl, cnt, ai ? 1u : 0u, lane);
     }
   }
 }
 
 // One hub chunk (k_heavy, one warp): relax arcs [first, end) of vertex v for
 // the pending groups recorded by k_light.  Same relaxation as sssp_task.
-__device__ void hub_chunk(const QDev* __restrict__ qd, const uint4 item, const GraphDev& g, uint32_t lane) {
+__device__ void hub_chunk(const QDev* __restrict__ qd, const uint4 item, const GraphDev& g, uint32_t lane,
+                          RelaxHdr* __restrict__ sh) {
   const unsigned FULL = 0xFFFFFFFFu;
-  const uint32_t slot = item.x & 0xFFFFu, rm = item.x >> 16, v = item.y;
+  if (item.z >= item.w) return;  // filler entry of a chunk run that did not fit
+  const uint32_t slot = item.x & 0xFFFFu, v = item.y;
   const QDev& q = qd[slot];
-  const uint32_t V = q.nv;
-  const uint32_t dj = lane < 8 ? ld_cg(q.dist + (size_t)v * 8 + lane) : INF32;
-  uint32_t d[KMAX];
-#pragma unroll
-  for (int t = 0; t < KMAX; t++) d[t] = __shfl_sync(FULL, dj, t);
-  const uint32_t best = __shfl_sync(FULL, ld_cg(&q.ctl->best), 0);
-  const uint32_t capb = (uint32_t)((unsigned long long)best * q.cap_num / q.cap_den);
-  uint32_t dmin = INF32;
-#pragma unroll
-  for (int t = 0; t < KMAX; t++)
-    if ((rm >> t) & 1u) dmin = min(dmin, d[t]);
-  if (dmin > capb) return;
-  const uint32_t lim = capb - dmin, thi = q.theta_hi;
-  uint32_t* pnext = q.sflag + (size_t)(q.par ^ 1u) * V;
-  uint32_t* pfar = q.sflag + (size_t)2 * V;
-  uint32_t n_arcs = 0, n_upd = 0, n_enq = 0;
-  for (uint32_t a0 = item.z; a0 < item.w; a0 += 32) {
-    uint32_t a = a0 + lane;
-    bool in = a < item.w;
-    uint2 arc = in ? __ldg(g.adj + a) : make_uint2(0, 0xFFFFFFFFu);
-    bool over = in && arc.y > lim;
-    bool takeN = false, takeF = false;
-    if (in && !over) {
-      n_arcs++;
-      const uint32_t u = arc.x;
-      const uint4* row = reinterpret_cast<const uint4*>(q.dist + (size_t)u * 8);
-      uint4 ra = __ldcg(row), rb = __ldcg(row + 1);
-      uint32_t du[8] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
-      uint32_t nn = 0, nf = 0;
-#pragma unroll
-      for (int t = 0; t < KMAX; t++) {
-        if ((rm >> t) & 1u) {
-          uint32_t nd = d[t] + arc.y;
-          if (nd <= capb && nd < du[t]) {
-            atomicMin(q.dist + (size_t)u * 8 + t, nd);
-            if (nd < thi)
-              nn |= 1u << t;
-            else
-              nf |= 1u << t;
-            n_upd++;
-          }
-        }
-      }
-      if (nn) takeN = atomicOr(pnext + u, nn) == 0u;
-      if (nf) takeF = atomicOr(pfar + u, nf) == 0u;
-    }
-    append_multi(takeN, arc.x, true, q, slot, lane, n_enq);
-    append_multi(takeF, arc.x, false, q, slot, lane, n_enq);
-    if (__any_sync(FULL, over)) break;
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    n_arcs += __shfl_xor_sync(FULL, n_arcs, o);
-    n_upd += __shfl_xor_sync(FULL, n_upd, o);
-    n_enq += __shfl_xor_sync(FULL, n_enq, o);
-  }
+  uint32_t capb = 0, n = 0;
   if (lane == 0) {
-    if (n_arcs) atomicAdd(&q.ctl->stat[ST_SSSP_ARCS], (unsigned long long)n_arcs);
-    if (n_upd) atomicAdd(&q.ctl->stat[ST_SSSP_UPDATES], (unsigned long long)n_upd);
-    if (n_enq) atomicAdd(&q.ctl->stat[ST_SSSP_ENQ], (unsigned long long)n_enq);
+    const uint4* drow = reinterpret_cast<const uint4*>(q.dist + (size_t)v * 8);
+    const uint4 da = __ldcg(drow), db = __ldcg(drow + 1);
+    const uint32_t best = ld_cg(&q.ctl->best);
+    const uint32_t d[8] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z, db.w};
+    capb = (uint32_t)((unsigned long long)best * q.cap_num / q.cap_den);
+    uint32_t rm = 0, dmin = INF32;
+#pragma unroll
+    for (int t = 0; t < KMAX; t++)
+      if (((item.x >> (16 + t)) & 1u) && d[t] <= capb) {
+        rm |= 1u << t;
+        dmin = min(dmin, d[t]);
+      }
+    RelaxHdr hd;
+#pragma unroll
+    for (int t = 0; t < KMAX; t++) hd.d[t] = d[t];
+    hd.rm = rm;
+    hd.lim = rm ? capb - dmin : 0u;
+    hd.a0 = item.z;
+    hd.pad = 0;
+    sh[0] = hd;
+    n = rm ? item.w - item.z : 0u;
   }
+  __syncwarp();
+  capb = __shfl_sync(FULL, capb, 0);
+  n = __shfl_sync(FULL, n, 0);
+  if (n == 0) return;
+  RelaxCnt cnt;
+  const uint32_t e1[1] = {n};
+  relax_flat<1>(q, sh, e1, capb, g, lane, cnt);
+  relax_cnt_flush(q.ctl, cnt, 0u, lane);
 }
 
 // Near-far split of one far item: cost in [theta_lo, theta_hi) -> near list;
@@ -1055,7 +1185,7 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
     if (tid <= nslots) pre[t * (MAX_SLOTS + 1) + tid] = before;
   }
   if (tid == 0) {
-    const uint32_t per_task[NT] = {32, 32, 32, 1, 1, 4, 4, 1, 1};
+    const uint32_t per_task[NT] = {32, 32, 32, 1, 1, SSSP_W, 4, 1, 1};
     uint32_t off = 0;
     for (int t = 0; t < NT; t++) {
       uint32_t tot = wsum[(blockDim.x >> 5) - 1][t];
@@ -1079,7 +1209,7 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
 // ---------------------------------------------------------------------------
 // Light round kernel: warp tasks of types T_SPLIT .. T_SSSP.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_light(const QDev* __restrict__ qd, RoundDesc* __restrict__ rd,
+__global__ void __launch_bounds__(256, 3) k_light(const QDev* __restrict__ qd, RoundDesc* __restrict__ rd,
                                                const uint32_t* __restrict__ pre, int nslots, GraphDev g) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1087,9 +1217,10 @@ __global__ void __launch_bounds__(256) k_light(const QDev* __restrict__ qd, Roun
   const uint32_t ntasks = __ldcg(&rd->light_tasks);
   // the distance items' prefix over slots, staged once per block
   __shared__ uint32_t s_pre[MAX_SLOTS + 1];
+  __shared__ RelaxHdr s_hdr[8][SSSP_W];
   for (int i = threadIdx.x; i <= nslots; i += blockDim.x) s_pre[i] = __ldcg(pre + T_SSSP * (MAX_SLOTS + 1) + i);
   __syncthreads();
-  SsspCounters sc;
+  SsspAcc acc;
   for (uint32_t task = warp; task < ntasks; task += nwarps) {
     int t = 0;
     while (t < T_SSSP && task >= __ldcg(&rd->task_off[t + 1])) t++;
@@ -1097,7 +1228,7 @@ __global__ void __launch_bounds__(256) k_light(const QDev* __restrict__ qd, Roun
     const uint32_t* P = pre + t * (MAX_SLOTS + 1);
     const uint32_t total = __ldcg(&rd->items[t]);
     if (t == T_SSSP) {
-      sssp_task(qd, s_pre, nslots, total, local, g, lane, sc, rd);
+      sssp_task(qd, s_pre, nslots, total, local, g, lane, acc, rd, s_hdr[threadIdx.x >> 5]);
     } else if (t == T_TOUR) {
       tour_warp(qd[find_slot(P, nslots, local)], lane);
     } else if (t == T_EXTRACT) {
@@ -1117,7 +1248,7 @@ __global__ void __launch_bounds__(256) k_light(const QDev* __restrict__ qd, Roun
       }
     }
   }
-  sssp_flush(sc, lane & 7u);
+  if (lane == 0) sssp_acc_flush(acc);
 }
 
 // Heavy round kernel: lower-bound table rows (one vertex per lane), then one
@@ -1132,6 +1263,7 @@ __global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, cons
   const uint32_t ntasks = __ldcg(&rd->heavy_tasks) + nbig;
   const uint32_t dp0 = __ldcg(&rd->task_off[T_DP]) + nbig, hop0 = __ldcg(&rd->task_off[T_HOP]) + nbig;
   __shared__ uint32_t s_dp[MAX_SLOTS + 1], s_hop[MAX_SLOTS + 1], s_lb[MAX_SLOTS + 1];
+  __shared__ RelaxHdr s_hub[8];
   for (int i = threadIdx.x; i <= nslots; i += blockDim.x) {
     s_dp[i] = __ldcg(pre + T_DP * (MAX_SLOTS + 1) + i);
     s_hop[i] = __ldcg(pre + T_HOP * (MAX_SLOTS + 1) + i);
@@ -1140,7 +1272,7 @@ __global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, cons
   __syncthreads();
   for (uint32_t task = warp; task < ntasks; task += nwarps) {
     if (task < nbig) {
-      hub_chunk(qd, __ldcg(rd->big + task), g, lane);
+      hub_chunk(qd, __ldcg(rd->big + task), g, lane, &s_hub[threadIdx.x >> 5]);
       continue;
     }
     if (task < dp0) {  // lower-bound table rows, 8 lanes per vertex
