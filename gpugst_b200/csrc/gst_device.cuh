@@ -32,9 +32,10 @@ constexpr int DMAX = 7;
 enum JobState : int32_t { J_FREE = 0, J_INIT, J_SSSP, J_TOUR, J_LB, J_DPSEED, J_DP, J_EXTRACT, J_DONE };
 enum Action : int32_t { A_NONE = 0, A_SSEED, A_WORK, A_SPLIT, A_TOUR, A_LB, A_DSEED, A_EXTRACT };
 
-// Task types of one round.  Light kernel: split, seeds, tour, extract and
-// distance items; heavy kernel: lower-bound tables and DP items.
-enum TaskType : int32_t { T_SPLIT = 0, T_SSEED, T_DSEED, T_TOUR, T_EXTRACT, T_SSSP, T_LB, T_DP, T_HOP, NT };
+// Task types of one round.  Light kernel: split, seeds, tour, extract,
+// distance items and DP states; heavy kernel: the arc chunks the light kernel
+// handed over, then lower-bound table rows.
+enum TaskType : int32_t { T_SPLIT = 0, T_SSEED, T_DSEED, T_TOUR, T_EXTRACT, T_SSSP, T_DP, T_HOP, T_LB, NT };
 constexpr int MAX_SLOTS = 1024;
 
 // Round-wide work description written by k_control.
@@ -43,15 +44,18 @@ struct RoundDesc {
   uint32_t task_off[NT + 1];  // warp-task offsets (light types, then heavy types restart at 0)
   uint32_t light_tasks, heavy_tasks;
   uint32_t n_live;        // slots whose job is not finished
-  uint32_t n_big;         // hub arc chunks queued by k_light for k_heavy this round
-  // hub arc chunks: {slot | groups << 16, vertex, first arc, end arc}; set
-  // once by the host (null / 0 disables chunking)
+  uint32_t n_big;         // arc chunks queued by k_light for k_heavy this round
+  // arc chunks: distance items {slot | groups << 16, vertex, first arc, end arc},
+  // DP grow chunks {slot | 1 << 31 (| 1 << 30 hop-bounded), state, first arc,
+  // end arc}; set once by the host (null / 0 disables chunking)
   uint4* big;
   uint32_t big_cap;
   uint32_t hub_min_deg;   // only items with at least this many arcs under their limit are chunked
   uint32_t hub_min_rest;  // ... and only when at least this many arcs remain under the limit
   uint32_t hub_max_items; // chunk only in rounds with fewer distance items (latency-bound rounds)
   uint32_t hub_on;        // set by k_control for the current round
+  uint32_t sssp_w;        // distance items per warp task this round (set by k_control)
+  uint32_t light_warps;   // warps of one k_light launch (set by the host)
   uint32_t pad3;
 };
 constexpr uint32_t HUB_CHUNK = 256;     // arcs per chunk (one warp)

@@ -297,6 +297,14 @@ class Runner {
     CK(cudaMalloc(&d_ctl_, MAX_SLOTS * sizeof(QCtl)));
     CK(cudaMalloc(&d_rd_, sizeof(RoundDesc)));
     {
+      // grids: every SM filled to the occupancy limit of each kernel
+      int bl = 0, bh = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, k_light, 256, 0));
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bh, k_heavy, 256, 0));
+      light_grid_ = (unsigned)g_->num_sms * (unsigned)std::max(1, bl);
+      heavy_grid_ = (unsigned)g_->num_sms * (unsigned)std::max(1, bh);
+    }
+    {
       // hub arc chunk list (k_light -> k_heavy within a round)
       big_cap_ = std::max(1u << 12, env_u32("GSTB_HUB_CHUNKS", 1u << 20));
       CK(cudaMalloc(&d_big_, (size_t)big_cap_ * sizeof(uint4)));
@@ -307,6 +315,8 @@ class Runner {
       rd.hub_min_deg = env_u32("GSTB_HUB_MIN_DEG", 256);
       rd.hub_min_rest = env_u32("GSTB_HUB_MIN_REST", 128);
       rd.hub_max_items = env_u32("GSTB_HUB_MAX_ITEMS", 1000000);
+      rd.light_warps = light_grid_ * (256 / 32);
+      rd.sssp_w = 4;
       CK(cudaMemcpy(d_rd_, &rd, sizeof(rd), cudaMemcpyHostToDevice));
     }
     CK(cudaMalloc(&d_pre_, (size_t)NT * (MAX_SLOTS + 1) * 4));
@@ -324,11 +334,6 @@ class Runner {
     CK(cudaMallocHost(&h_edge_stage_, edge_stage_cap_));
     memset(h_qd_, 0, sizeof(QDev));  // the zero descriptor that frees a slot
     slots_.assign(max_slots_, nullptr);
-    int bl = 0, bh = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, k_light, 256, 0));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bh, k_heavy, 256, 0));
-    light_grid_ = (unsigned)g_->num_sms * (unsigned)std::max(1, bl);
-    heavy_grid_ = (unsigned)g_->num_sms * (unsigned)std::max(1, bh);
     return GST_OK;
   }
 
@@ -1272,7 +1277,19 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   CK(cudaMemsetAsync(q.dist, 0xFF, (size_t)g->V * 8 * 4, 0));
   CK(cudaMemsetAsync(q.dflag, 0, L.sflag - L.dflag, 0));
   CK(cudaMemsetAsync(q.sflag, 0, L.qbuf - L.sflag, 0));
-  CK(cudaMemsetAsync(d_rd, 0, sizeof(RoundDesc), 0));
+  // grids: every SM filled to the occupancy limit of each kernel
+  int bl = 0, bh = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, k_light, 256, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bh, k_heavy, 256, 0));
+  const unsigned light_grid = (unsigned)g->num_sms * (unsigned)std::max(1, bl);
+  const unsigned heavy_grid = (unsigned)g->num_sms * (unsigned)std::max(1, bh);
+  {
+    RoundDesc rd0;  // no arc chunk list: chunking stays off
+    memset(&rd0, 0, sizeof(rd0));
+    rd0.light_warps = light_grid * (256 / 32);
+    rd0.sssp_w = 4;
+    CK(cudaMemcpy(d_rd, &rd0, sizeof(RoundDesc), cudaMemcpyHostToDevice));
+  }
   // member items v*8 + j, staged through a fixed host buffer
   {
     uint32_t stage[1024];
@@ -1293,7 +1310,6 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   CK(cudaMemcpy(d_ctl, &c, sizeof(QCtl), cudaMemcpyHostToDevice));
 
   GraphDev gd{g->d_beg, g->d_adj, g->V, g->d_wcut};
-  const unsigned light_grid = (unsigned)g->num_sms * 4, heavy_grid = (unsigned)g->num_sms * 2;
   const uint32_t R = 6;
   const uint64_t max_rounds = 1ull << 22;
   uint64_t rounds = 0;

@@ -5,17 +5,18 @@
 //   k_control  one thread per query slot: advances the query's state machine
 //              (distance rounds -> tour tables -> DP seed -> DP rounds ->
 //              extraction) and writes the round's work description;
-//   k_light    warp tasks: near-far splits, seeds, tour tables, extraction and
+//   k_light    warp tasks: near-far splits, seeds, tour tables, extraction,
 //              distance items (a vertex with its pending groups; the arcs of
 //              a task's items are relaxed as one flat list by the whole warp:
-//              multi-source relax, replacing dis0_init_1, DPQ.cu:241-271);
-//   k_heavy    warp per DP state:
-//                   DP item       : best update from complement / one-label
-//                                   completion, lower-bound prune, grow along
-//                                   the weight-sorted adjacency, merge with
-//                                   every disjoint subset at the vertex
-//                                   (replaces Relax, DPQ.cu:73-172 and
-//                                   D-GPUGST/src/DPQ.cu:62-126)
+//              multi-source relax, replacing dis0_init_1, DPQ.cu:241-271) and
+//              DP items, one warp per state: best update from complement /
+//              one-label completion, lower-bound prune, grow along the
+//              weight-sorted adjacency, merge with every disjoint subset at
+//              the vertex (replaces Relax, DPQ.cu:73-172 and
+//              D-GPUGST/src/DPQ.cu:62-126);
+//   k_heavy    the arc chunks k_light handed over in the same round (hub
+//              vertices of distance items, high-degree DP states), then
+//              lower-bound table rows;
 //   split      near-far bucketing: far items whose cost entered the new
 //              window move to the near list
 //   tour       group-to-group distances and tour tables (host DP at
@@ -28,6 +29,12 @@
 #include "gst_device.cuh"
 
 namespace gstb {
+
+__device__ __forceinline__ uint32_t warp_sum(uint32_t x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, o);
+  return x;
+}
 
 // ---------------------------------------------------------------------------
 // Warp-aggregated enqueue.  Every lane of the warp calls it (want may be
@@ -99,6 +106,157 @@ __device__ __forceinline__ void append_multi(bool take, uint32_t item, bool near
   }
 }
 
+// Warp-wide append of up to U items per lane to the near-out and far lists
+// of one query: one reservation per list and warp, then plain stores.  Every
+// lane of the warp calls it; returns this lane's number of appended items.
+template <int U>
+__device__ __forceinline__ uint32_t append_lists(const bool (&takeN)[U], const bool (&takeF)[U],
+                                                 const uint32_t (&item)[U], const QDev& q, uint32_t lane) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  uint32_t cN = 0, cF = 0;
+#pragma unroll
+  for (int u = 0; u < U; u++) {
+    cN += takeN[u] ? 1u : 0u;
+    cF += takeF[u] ? 1u : 0u;
+  }
+  if (!__any_sync(FULL, (cN | cF) != 0u)) return 0u;
+  uint32_t xN = cN, xF = cF;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t yN = __shfl_up_sync(FULL, xN, o), yF = __shfl_up_sync(FULL, xF, o);
+    if (lane >= (uint32_t)o) {
+      xN += yN;
+      xF += yF;
+    }
+  }
+  const uint32_t totN = __shfl_sync(FULL, xN, 31), totF = __shfl_sync(FULL, xF, 31);
+  uint32_t bN = 0, bF = 0;
+  if (lane == 0) {
+    if (totN) bN = atomicAdd(&q.ctl->n_near, totN);
+    if (totF) bF = atomicAdd(&q.ctl->n_far, totF);
+  }
+  uint32_t pN = __shfl_sync(FULL, bN, 0) + xN - cN, pF = __shfl_sync(FULL, bF, 0) + xF - cF;
+  uint32_t* outN = q.qbuf[q.out_idx];
+  uint32_t* outF = q.qbuf[q.far_idx];
+  bool ovf = false;
+#pragma unroll
+  for (int u = 0; u < U; u++) {
+    if (takeN[u]) {
+      if (pN < q.cap)
+        outN[pN] = item[u];
+      else
+        ovf = true;
+      pN++;
+    }
+    if (takeF[u]) {
+      if (pF < q.cap)
+        outF[pF] = item[u];
+      else
+        ovf = true;
+      pF++;
+    }
+  }
+  if (ovf) atomicExch(&q.ctl->overflow, 1u);
+  return cN + cF;
+}
+
+// ---------------------------------------------------------------------------
+// Grow of one DP state (v, p) -- or (v, p, d) with target hop count d+1 --
+// along its arcs [a0, a1): target (u, p[, d+1]) at cost c + w(v, u).  GROW_U
+// arcs per lane per step, so every lane keeps GROW_U independent chains
+// (arc -> target word and bound -> flag) in flight.  A target is lowered
+// with a fire-and-forget 64-bit min after a pre-check against its cost and
+// the bound check; its state flag gates the list entry.
+// ---------------------------------------------------------------------------
+#ifndef GSTB_GROW_U
+#define GSTB_GROW_U 4
+#endif
+constexpr int GROW_U = GSTB_GROW_U;
+constexpr uint32_t GROW_LOCAL = 32u * GROW_U;  // arcs a state grows itself; the rest go out in chunks
+
+struct GrowCnt {
+  uint32_t arcs = 0, upd = 0, enq = 0;
+};
+
+__device__ __forceinline__ void grow_arcs(const QDev& q, const GraphDev& g, uint32_t lane, uint32_t v, uint32_t p,
+                                          uint32_t comp, uint32_t c, uint32_t best, uint32_t lim, int dnext,
+                                          uint32_t a0, uint32_t a1, GrowCnt& cnt) {
+  const int k = q.k;
+  const uint32_t nd = (uint32_t)q.nd, thi = q.theta_hi, par = q.par;
+  const unsigned short* __restrict__ lbt = q.lbt;
+  for (uint32_t base = a0; base < a1; base += 32u * GROW_U) {
+    uint2 arc[GROW_U];
+    bool ok[GROW_U];
+#pragma unroll
+    for (int u = 0; u < GROW_U; u++) {
+      const uint32_t a = base + (uint32_t)u * 32u + lane;
+      ok[u] = a < a1;
+      arc[u] = ok[u] ? __ldg(g.adj + a) : make_uint2(0u, 0u);
+    }
+    uint32_t t[GROW_U], cur[GROW_U], lbu[GROW_U];
+#pragma unroll
+    for (int u = 0; u < GROW_U; u++) {
+      ok[u] = ok[u] && arc[u].y <= lim;
+      const uint32_t vp = (arc[u].x << k) | p;
+      t[u] = dnext < 0 ? vp : vp * nd + (uint32_t)dnext;
+      cur[u] = ok[u] ? (uint32_t)(ld_cg(q.table + t[u]) >> 32) : 0u;
+      lbu[u] = ok[u] ? (uint32_t)__ldg(lbt + ((size_t)arc[u].x << k) + comp) : 0u;
+    }
+    bool want[GROW_U];
+    uint32_t nc[GROW_U];
+#pragma unroll
+    for (int u = 0; u < GROW_U; u++) {
+      nc[u] = c + arc[u].y;
+      want[u] = ok[u] && nc[u] < cur[u] && (unsigned long long)nc[u] + lbu[u] <= best;
+      if (ok[u]) cnt.arcs++;
+      if (want[u]) {
+        // the pre-check already saw a higher cost: enqueue on it and let the
+        // 64-bit min land without waiting for its result (a concurrent lower
+        // write also enqueues; the flag keeps the list free of duplicates)
+        atomicMin(q.table + t[u], pack(nc[u], PAR_GROW | v));
+        cnt.upd++;
+      }
+    }
+    // near entries are flagged with the next round's parity, far ones with bit 2
+    uint32_t old[GROW_U], bit[GROW_U];
+#pragma unroll
+    for (int u = 0; u < GROW_U; u++) {
+      bit[u] = dflag_bit(t[u], nc[u] < thi ? (par ^ 1u) : 2u);
+      old[u] = want[u] ? atomicOr(&q.dflag[t[u] >> 3], bit[u]) : bit[u];
+    }
+    bool tN[GROW_U], tF[GROW_U];
+#pragma unroll
+    for (int u = 0; u < GROW_U; u++) {
+      const bool take = !(old[u] & bit[u]);
+      tN[u] = take && nc[u] < thi;
+      tF[u] = take && !(nc[u] < thi);
+    }
+    cnt.enq += append_lists<GROW_U>(tN, tF, t, q, lane);
+  }
+}
+
+// A warp hands the arcs [a0, a1) of a state's grow to k_heavy in HUB_CHUNK
+// pieces.  Entries below the list's capacity are always written (empty
+// ranges when the run does not fit), so k_heavy never reads a stale entry.
+// Returns false if the run did not fit: the caller then grows those arcs.
+constexpr uint32_t CH_GROW = 1u << 31;  // big-list entry is a DP grow chunk
+constexpr uint32_t CH_HOP = 1u << 30;   // ... of a hop-bounded state
+
+__device__ __forceinline__ bool push_grow_chunks(RoundDesc* rd, uint32_t slot, bool hop, uint32_t s, uint32_t a0,
+                                                 uint32_t a1, uint32_t lane) {
+  const uint32_t nch = (a1 - a0 + HUB_CHUNK - 1u) / HUB_CHUNK;
+  uint32_t cb = 0;
+  if (lane == 0) cb = atomicAdd(&rd->n_big, nch);
+  cb = __shfl_sync(0xFFFFFFFFu, cb, 0);
+  const bool fits = cb + nch <= rd->big_cap;
+  const uint32_t x = slot | CH_GROW | (hop ? CH_HOP : 0u);
+  for (uint32_t c = lane; c < nch && cb + c < rd->big_cap; c += 32u) {
+    const uint32_t s0 = a0 + c * HUB_CHUNK;
+    rd->big[cb + c] = fits ? make_uint4(x, s, s0, min(s0 + HUB_CHUNK, a1)) : make_uint4(slot, 0u, 0u, 0u);
+  }
+  return fits;
+}
+
 // Load the capped group distances of vertex v into every lane's registers.
 __device__ __forceinline__ void load_dl(const QDev& q, uint32_t v, uint32_t (&dl)[KMAX],
                                         uint32_t& raw_sum_ok, uint32_t comp,
@@ -121,7 +279,8 @@ __device__ __forceinline__ void load_dl(const QDev& q, uint32_t v, uint32_t (&dl
 // ---------------------------------------------------------------------------
 // Unbounded DP item (v, p).
 // ---------------------------------------------------------------------------
-__device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t lane) {
+__device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t lane, RoundDesc* __restrict__ rd,
+                        uint32_t slot) {
   const unsigned FULL = 0xFFFFFFFFu;
   const int k = q.k;
   const uint32_t K2 = 1u << k, full = (uint32_t)q.full;
@@ -165,38 +324,23 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
   uint32_t lbv = __ldg(lbt + ((size_t)v << k) + comp);
   if ((unsigned long long)c + lbv > best) return;
 
-  uint32_t scanned = 0, upd = 0;
+  GrowCnt gc;
   // grow, only from states of cost <= best/2 (optimal-tree decomposition,
-  // CPUNONHOP.h:820; exact for the unbounded problem, see DESIGN)
+  // CPUNONHOP.h:820; exact for the unbounded problem); a high-degree vertex
+  // grows its first GROW_LOCAL arcs here and hands the rest to k_heavy
   if (2ull * c <= best) {
-    uint32_t lim = best - c;
-    uint32_t a0 = __ldg(g.beg + v), a1 = arcs_upto(g, v, __ldg(g.beg + v + 1), lim);
-    for (uint32_t base = a0; base < a1; base += 32) {
-      uint32_t a = base + lane;
-      bool in = a < a1;
-      uint2 arc = in ? __ldg(g.adj + a) : make_uint2(0, 0xFFFFFFFFu);
-      bool over = arc.y > lim;
-      bool want = false;
-      uint32_t t = 0, nc = 0;
-      if (in && !over) {
-        scanned++;
-        nc = c + arc.y;
-        t = (arc.x << k) | p;
-        if (nc < (uint32_t)(ld_cg(q.table + t) >> 32)) {
-          uint32_t lbu = __ldg(lbt + ((size_t)arc.x << k) + comp);
-          if ((unsigned long long)nc + lbu <= best) {
-            // the pre-check already saw a higher cost: enqueue on it and let the
-            // 64-bit min land without waiting for its result (a concurrent lower
-            // write also enqueues; the flag keeps the list free of duplicates)
-            atomicMin(q.table + t, pack(nc, PAR_GROW | v));
-            want = true;
-            upd += want;
-          }
-        }
-      }
-      enqueue_warp(want, t, nc, q, q.dflag, lane);
-      if (__any_sync(FULL, over)) break;
-    }
+    const uint32_t lim = best - c;
+    const uint32_t a0 = __ldg(g.beg + v);
+    uint32_t a1 = arcs_upto(g, v, __ldg(g.beg + v + 1), lim);
+    if (rd->hub_on && a1 - a0 >= rd->hub_min_deg &&
+        push_grow_chunks(rd, slot, false, s, a0 + GROW_LOCAL, a1, lane))
+      a1 = a0 + GROW_LOCAL;
+    grow_arcs(q, g, lane, v, p, comp, c, best, lim, -1, a0, a1, gc);
+  }
+  uint32_t scanned = gc.arcs, upd = gc.upd;
+  {
+    const uint32_t e = warp_sum(gc.enq);
+    if (lane == 0 && e) atomicAdd(&q.ctl->stat[ST_ENQ], (unsigned long long)e);
   }
   // merge with every proper, non-empty subset p2 of the complement
   // (DPQ.cu:140-170; the complement itself went to the full state above)
@@ -248,7 +392,8 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
 // ---------------------------------------------------------------------------
 // Hop-bounded DP item (v, p, d): state id ((v << k) | p) * nd + d.
 // ---------------------------------------------------------------------------
-__device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t lane) {
+__device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t lane, RoundDesc* __restrict__ rd,
+                         uint32_t slot) {
   const unsigned FULL = 0xFFFFFFFFu;
   const int k = q.k, nd = q.nd, D = q.D;
   const uint32_t K2 = 1u << k, full = (uint32_t)q.full;
@@ -274,36 +419,20 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
   const unsigned short* lbt = q.lbt;
   uint32_t lbv = __ldg(lbt + ((size_t)v << k) + comp);
   if ((unsigned long long)c + lbv > best) return;
-  uint32_t scanned = 0, upd = 0;
+  GrowCnt gc;
   if (d < (uint32_t)D) {  // grow d -> d+1 (CPUHOP.h:192-206)
-    uint32_t lim = best - c;
-    uint32_t a0 = __ldg(g.beg + v), a1 = arcs_upto(g, v, __ldg(g.beg + v + 1), lim);
-    for (uint32_t base = a0; base < a1; base += 32) {
-      uint32_t a = base + lane;
-      bool in = a < a1;
-      uint2 arc = in ? __ldg(g.adj + a) : make_uint2(0, 0xFFFFFFFFu);
-      bool over = arc.y > lim;
-      bool want = false;
-      uint32_t t = 0, nc = 0;
-      if (in && !over) {
-        scanned++;
-        nc = c + arc.y;
-        t = ((arc.x << k) | p) * (uint32_t)nd + d + 1;
-        if (nc < (uint32_t)(ld_cg(q.table + t) >> 32)) {
-          uint32_t lbu = __ldg(lbt + ((size_t)arc.x << k) + comp);
-          if ((unsigned long long)nc + lbu <= best) {
-            // the pre-check already saw a higher cost: enqueue on it and let the
-            // 64-bit min land without waiting for its result (a concurrent lower
-            // write also enqueues; the flag keeps the list free of duplicates)
-            atomicMin(q.table + t, pack(nc, PAR_GROW | v));
-            want = true;
-            upd += want;
-          }
-        }
-      }
-      enqueue_warp(want, t, nc, q, q.dflag, lane);
-      if (__any_sync(FULL, over)) break;
-    }
+    const uint32_t lim = best - c;
+    const uint32_t a0 = __ldg(g.beg + v);
+    uint32_t a1 = arcs_upto(g, v, __ldg(g.beg + v + 1), lim);
+    if (rd->hub_on && a1 - a0 >= rd->hub_min_deg &&
+        push_grow_chunks(rd, slot, true, s, a0 + GROW_LOCAL, a1, lane))
+      a1 = a0 + GROW_LOCAL;
+    grow_arcs(q, g, lane, v, p, comp, c, best, lim, (int)d + 1, a0, a1, gc);
+  }
+  uint32_t scanned = gc.arcs, upd = gc.upd;
+  {
+    const uint32_t e = warp_sum(gc.enq);
+    if (lane == 0 && e) atomicAdd(&q.ctl->stat[ST_ENQ], (unsigned long long)e);
   }
   // merge with (v, p2, d2), p2 a non-empty subset of the complement,
   // d2 <= D - d, into (v, p|p2, max(d, d2))  (CPUHOP.h:208-227)
@@ -389,15 +518,20 @@ __device__ __forceinline__ uint32_t find_slot_s(const uint32_t* pre, int nslots,
 }
 
 // ---------------------------------------------------------------------------
-// Distance items.  A warp task holds up to SSSP_W items (a vertex with the
-// mask of its pending groups).  Lanes 0..SSSP_W-1 read the items' headers in
-// parallel; then the arcs of all items of the task are relaxed as one flat
-// list, 32 x SSSP_U arcs per step.  Each lane keeps SSSP_U independent
-// chains (arc -> distance row -> pending flag) in flight, and uneven degrees
-// are spread over all 32 lanes instead of one lane group per item.
+// Distance items.  A warp task holds W items (a vertex with the mask of its
+// pending groups); W is chosen per round by k_control: 4 when the round has
+// few items (short rounds, low latency), up to 32 when it has many (fewer
+// per-task overheads).  Lanes 0..W-1 read the items' headers in parallel;
+// then the arcs of all items of one query in the task are relaxed as one flat
+// list, 32 x SSSP_U arcs per step.  Each lane keeps SSSP_U independent chains
+// (arc -> distance row -> pending flag) in flight, and uneven degrees are
+// spread over all 32 lanes.
 // ---------------------------------------------------------------------------
-constexpr int SSSP_W = 4;            // items per warp task (k_control's per-task count)
-constexpr int SSSP_U = 4;            // arcs per lane per step
+constexpr uint32_t SSSP_WMAX = 32;   // most items per warp task
+#ifndef GSTB_SSSP_U
+#define GSTB_SSSP_U 4
+#endif
+constexpr int SSSP_U = GSTB_SSSP_U;  // arcs per lane per step
 constexpr uint32_t HUB_LOCAL = 32;   // arcs of a hub item its own task relaxes
 
 struct alignas(16) RelaxHdr {
@@ -429,50 +563,51 @@ __device__ __forceinline__ void sssp_acc_flush(SsspAcc& a) {
   a.items = a.arcs = a.upd = a.enq = 0;
 }
 
-__device__ __forceinline__ uint32_t warp_sum(uint32_t x) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, o);
-  return x;
-}
-
 __device__ __forceinline__ uint32_t sel8(const uint4& a, const uint4& b, uint32_t i) {
   const uint4& h = i < 4u ? a : b;
   const uint32_t j = i & 3u;
   return j == 0u ? h.x : (j == 1u ? h.y : (j == 2u ? h.z : h.w));
 }
 
-// Relax the arcs [h[i].a0, h[i].a0 + n_i) of W items of query q, where
-// ends[i] = n_0 + ... + n_i (warp-uniform).  Every lane of the warp calls it.
-// A lowered distance is written with a fire-and-forget atomicMin after a
-// pre-check; the pending-groups flag of the target gates its list entry
-// (parity-split flags, so no update is lost); appends are aggregated over
-// the whole warp.
-template <int W>
-__device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __restrict__ h, const uint32_t (&ends)[W],
-                                           uint32_t capb, const GraphDev& g, uint32_t lane, RelaxCnt& cnt) {
+// Relax the arcs of the task's items [i0, i1), all of query q.  Lane j holds
+// in `x` the inclusive prefix n_0 + ... + n_j of the task's arc counts; item
+// i's arcs are [h[i].a0, h[i].a0 + n_i).  Every lane of the warp calls it with
+// the same i0, i1.  A lowered distance is written with a fire-and-forget
+// atomicMin after a pre-check; the pending-groups flag of the target gates
+// its list entry (parity-split flags, so no update is lost); appends are
+// aggregated over the whole warp.
+__device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __restrict__ h, uint32_t x, uint32_t i0,
+                                           uint32_t i1, uint32_t capb, const GraphDev& g, uint32_t lane,
+                                           RelaxCnt& cnt) {
   const unsigned FULL = 0xFFFFFFFFu;
-  const uint32_t total = ends[W - 1];
+  const uint32_t lo_end = __shfl_sync(FULL, x, i0 == 0u ? 0u : i0 - 1u);
+  const uint32_t f0 = i0 == 0u ? 0u : lo_end;
+  const uint32_t f1 = __shfl_sync(FULL, x, i1 - 1u);
   const uint32_t V = q.nv, thi = q.theta_hi;
   uint32_t* __restrict__ dist = q.dist;
   uint32_t* pnext = q.sflag + (size_t)(q.par ^ 1u) * V;
   uint32_t* pfar = q.sflag + (size_t)2 * V;
-  for (uint32_t base = 0; base < total; base += 32u * SSSP_U) {
+  for (uint32_t base = f0; base < f1; base += 32u * SSSP_U) {
     uint2 arc[SSSP_U];
     uint32_t itm[SSSP_U];
     bool ok[SSSP_U];
 #pragma unroll
     for (int u = 0; u < SSSP_U; u++) {
       const uint32_t f = base + (uint32_t)u * 32u + lane;
-      uint32_t i = 0, start = 0;
+      // item of flat position f: the first i in [i0, i1) with x_i > f
+      // (binary lifting over the lanes' prefixes)
+      uint32_t pos = i0;
 #pragma unroll
-      for (int j = 0; j < W - 1; j++)
-        if (f >= ends[j]) {
-          i = (uint32_t)j + 1u;
-          start = ends[j];
-        }
-      itm[u] = i;
-      ok[u] = f < total;
-      arc[u] = ok[u] ? __ldg(g.adj + h[i].a0 + (f - start)) : make_uint2(0u, 0u);
+      for (uint32_t step = 16; step > 0; step >>= 1) {
+        const uint32_t cand = pos + step - 1u;
+        const uint32_t xc = __shfl_sync(FULL, x, min(cand, 31u));
+        if (cand < i1 && xc <= f) pos += step;
+      }
+      const uint32_t xs = __shfl_sync(FULL, x, pos == 0u ? 0u : min(pos - 1u, 31u));
+      const uint32_t start = pos == 0u ? 0u : xs;
+      ok[u] = f < f1;
+      itm[u] = ok[u] ? pos : i0;
+      arc[u] = ok[u] ? __ldg(g.adj + h[itm[u]].a0 + (f - start)) : make_uint2(0u, 0u);
     }
     uint4 ra[SSSP_U], rb[SSSP_U];
 #pragma unroll
@@ -513,58 +648,20 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
       }
     }
     // all flag updates of the step are issued before any result is used
-    uint32_t oN[SSSP_U], oF[SSSP_U];
+    uint32_t oN[SSSP_U], oF[SSSP_U], itv[SSSP_U];
 #pragma unroll
     for (int u = 0; u < SSSP_U; u++) {
       oN[u] = nn[u] ? atomicOr(pnext + arc[u].x, nn[u]) : 1u;
       oF[u] = nf[u] ? atomicOr(pfar + arc[u].x, nf[u]) : 1u;
+      itv[u] = arc[u].x;
     }
-    uint32_t cN = 0, cF = 0;
+    bool tN[SSSP_U], tF[SSSP_U];
 #pragma unroll
     for (int u = 0; u < SSSP_U; u++) {
-      cN += oN[u] == 0u;
-      cF += oF[u] == 0u;
+      tN[u] = oN[u] == 0u;
+      tF[u] = oF[u] == 0u;
     }
-    if (!__any_sync(FULL, (cN | cF) != 0u)) continue;
-    // one list reservation per warp and list
-    uint32_t xN = cN, xF = cF;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t yN = __shfl_up_sync(FULL, xN, o), yF = __shfl_up_sync(FULL, xF, o);
-      if (lane >= (uint32_t)o) {
-        xN += yN;
-        xF += yF;
-      }
-    }
-    const uint32_t totN = __shfl_sync(FULL, xN, 31), totF = __shfl_sync(FULL, xF, 31);
-    uint32_t bN = 0, bF = 0;
-    if (lane == 0) {
-      if (totN) bN = atomicAdd(&q.ctl->n_near, totN);
-      if (totF) bF = atomicAdd(&q.ctl->n_far, totF);
-    }
-    uint32_t pN = __shfl_sync(FULL, bN, 0) + xN - cN, pF = __shfl_sync(FULL, bF, 0) + xF - cF;
-    uint32_t* outN = q.qbuf[q.out_idx];
-    uint32_t* outF = q.qbuf[q.far_idx];
-    bool ovf = false;
-#pragma unroll
-    for (int u = 0; u < SSSP_U; u++) {
-      if (oN[u] == 0u) {
-        if (pN < q.cap)
-          outN[pN] = arc[u].x;
-        else
-          ovf = true;
-        pN++;
-      }
-      if (oF[u] == 0u) {
-        if (pF < q.cap)
-          outF[pF] = arc[u].x;
-        else
-          ovf = true;
-        pF++;
-      }
-    }
-    if (ovf) atomicExch(&q.ctl->overflow, 1u);
-    cnt.enq += cN + cF;
+    cnt.enq += append_lists<SSSP_U>(tN, tF, itv, q, lane);
   }
 }
 
@@ -579,11 +676,11 @@ __device__ __forceinline__ void relax_cnt_flush(QCtl* c, RelaxCnt cnt, uint32_t 
 }
 
 __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restrict__ pre, int nslots,
-                          uint32_t total, uint32_t task, const GraphDev& g, uint32_t lane, SsspAcc& acc,
+                          uint32_t total, uint32_t task, uint32_t W, const GraphDev& g, uint32_t lane, SsspAcc& acc,
                           RoundDesc* __restrict__ rd, RelaxHdr* __restrict__ sh) {
   const unsigned FULL = 0xFFFFFFFFu;
-  const uint32_t it = task * (uint32_t)SSSP_W + lane;
-  const bool valid = lane < (uint32_t)SSSP_W && it < total;
+  const uint32_t it = task * W + lane;
+  const bool valid = lane < W && it < total;
   const uint32_t slot = valid ? find_slot_s(pre, nslots, it) : 0xFFFFFFFFu;
   uint32_t n = 0, capb = INF32;
   bool active = false;
@@ -664,26 +761,33 @@ __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restric
     sh[lane] = hd;
   }
   __syncwarp();
-  const uint32_t slot0 = __shfl_sync(FULL, slot, 0);
-  if (slot0 == 0xFFFFFFFFu) return;
-  const uint32_t n_items = __popc(__ballot_sync(FULL, active));
-  if (__all_sync(FULL, !valid || slot == slot0)) {
-    // one query: the items' arcs form one flat list
-    uint32_t x = n;
+  // valid items are lanes [0, nvalid); split them into runs of one query
+  const unsigned vmask = __ballot_sync(FULL, valid);
+  if (vmask == 0u) return;
+  const uint32_t nvalid = 32u - __clz(vmask);
+  uint32_t x = n;  // inclusive prefix of the arc counts over the lanes
 #pragma unroll
-    for (int o = 1; o < SSSP_W; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(FULL, x, o);
-      if (lane >= (uint32_t)o) x += y;
-    }
-    uint32_t ends[SSSP_W];
-#pragma unroll
-    for (int j = 0; j < SSSP_W; j++) ends[j] = __shfl_sync(FULL, x, j);
-    uint32_t cb = capb;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(FULL, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  const uint32_t prev_slot = __shfl_up_sync(FULL, slot, 1);
+  unsigned runs = __ballot_sync(FULL, valid && (lane == 0u || prev_slot != slot));
+  const unsigned amask = __ballot_sync(FULL, active);
+  while (runs) {
+    const uint32_t i0 = (uint32_t)(__ffs(runs) - 1);
+    runs &= runs - 1u;
+    const uint32_t i1 = runs ? (uint32_t)(__ffs(runs) - 1) : nvalid;
+    const uint32_t si = __shfl_sync(FULL, slot, i0);
+    const bool in_run = lane >= i0 && lane < i1;
+    uint32_t cb = in_run ? capb : INF32;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cb = min(cb, __shfl_xor_sync(FULL, cb, o));
-    const QDev& q = qd[slot0];
+    const unsigned rmask = (i1 >= 32u ? 0xFFFFFFFFu : ((1u << i1) - 1u)) & ~((1u << i0) - 1u);
+    const uint32_t n_items = __popc(amask & rmask);
+    const QDev& q = qd[si];
     RelaxCnt cnt;
-    if (ends[SSSP_W - 1]) relax_flat<SSSP_W>(q, sh, ends, cb, g, lane, cnt);
+    relax_flat(q, sh, x, i0, i1, cb, g, lane, cnt);
     const uint32_t a = warp_sum(cnt.arcs), u = warp_sum(cnt.upd), e = warp_sum(cnt.enq);
     if (lane == 0) {
       if (acc.cur != q.ctl) {
@@ -694,20 +798,6 @@ __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restric
       acc.arcs += a;
       acc.upd += u;
       acc.enq += e;
-    }
-  } else {
-    // the task straddles queries (at most one task per query boundary and
-    // round): relax item by item
-    for (int i = 0; i < SSSP_W; i++) {
-      const uint32_t si = __shfl_sync(FULL, slot, i), ni = __shfl_sync(FULL, n, i);
-      const uint32_t ci = __shfl_sync(FULL, capb, i);
-      const bool ai = __shfl_sync(FULL, active, i);
-      if (si == 0xFFFFFFFFu) continue;
-      const QDev& q = qd[si];
-      RelaxCnt cnt;
-      const uint32_t e1[1] = {ni};
-      if (ni) relax_flat<1>(q, sh + i, e1, ci, g, lane, cnt);
-      relax_cnt_flush(q.ctl, cnt, ai ? 1u : 0u, lane);
     }
   }
 }
@@ -749,9 +839,43 @@ __device__ void hub_chunk(const QDev* __restrict__ qd, const uint4 item, const G
   n = __shfl_sync(FULL, n, 0);
   if (n == 0) return;
   RelaxCnt cnt;
-  const uint32_t e1[1] = {n};
-  relax_flat<1>(q, sh, e1, capb, g, lane, cnt);
+  relax_flat(q, sh, n, 0u, 1u, capb, g, lane, cnt);  // one item: every lane holds its prefix n
   relax_cnt_flush(q.ctl, cnt, 0u, lane);
+}
+
+// One DP grow chunk (k_heavy, one warp): arcs [first, end) of a state that a
+// k_light warp handed over.  The state's current cost is read again (it can
+// only have dropped, and a lower cost grows validly too) and the gates of the
+// state's own expansion are re-checked.
+__device__ void grow_chunk(const QDev* __restrict__ qd, const uint4 item, const GraphDev& g, uint32_t lane) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  if (item.z >= item.w) return;  // filler entry of a chunk run that did not fit
+  const uint32_t slot = item.x & 0xFFFFu;
+  const bool hop = (item.x & CH_HOP) != 0u;
+  const QDev& q = qd[slot];
+  const int k = q.k;
+  const uint32_t K2 = 1u << k, full = (uint32_t)q.full, nd = (uint32_t)q.nd, s = item.y;
+  const uint32_t vp = hop ? s / nd : s, d = hop ? s % nd : 0u;
+  const uint32_t v = vp >> k, p = vp & (K2 - 1u), comp = full ^ p;
+  uint32_t c = 0, best = 0, lbv = 0;
+  if (lane == 0) {
+    c = (uint32_t)(ld_cg(q.table + s) >> 32);
+    best = ld_cg(&q.ctl->best);
+    lbv = __ldg(q.lbt + ((size_t)v << k) + comp);
+  }
+  c = __shfl_sync(FULL, c, 0);
+  best = __shfl_sync(FULL, best, 0);
+  lbv = __shfl_sync(FULL, lbv, 0);
+  if (c == INF32 || c > best || (unsigned long long)c + lbv > best) return;
+  if (!hop && 2ull * c > best) return;
+  GrowCnt gc;
+  grow_arcs(q, g, lane, v, p, comp, c, best, best - c, hop ? (int)d + 1 : -1, item.z, item.w, gc);
+  const uint32_t a = warp_sum(gc.arcs), u = warp_sum(gc.upd), e = warp_sum(gc.enq);
+  if (lane == 0) {
+    if (a) atomicAdd(&q.ctl->stat[ST_ARCS], (unsigned long long)a);
+    if (u) atomicAdd(&q.ctl->stat[ST_UPDATES], (unsigned long long)u);
+    if (e) atomicAdd(&q.ctl->stat[ST_ENQ], (unsigned long long)e);
+  }
 }
 
 // Near-far split of one far item: cost in [theta_lo, theta_hi) -> near list;
@@ -1185,7 +1309,13 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
     if (tid <= nslots) pre[t * (MAX_SLOTS + 1) + tid] = before;
   }
   if (tid == 0) {
-    const uint32_t per_task[NT] = {32, 32, 32, 1, 1, SSSP_W, 4, 1, 1};
+    // distance items per warp task: 4 while that leaves at most two tasks per
+    // light warp, more (up to 32) in rounds with many items
+    uint32_t w = 4;
+    const unsigned long long n_sssp = wsum[(blockDim.x >> 5) - 1][T_SSSP];
+    while (w < SSSP_WMAX && n_sssp > 2ull * w * rd->light_warps) w <<= 1;
+    rd->sssp_w = w;
+    const uint32_t per_task[NT] = {32, 32, 32, 1, 1, w, 1, 1, 4};
     uint32_t off = 0;
     for (int t = 0; t < NT; t++) {
       uint32_t tot = wsum[(blockDim.x >> 5) - 1][t];
@@ -1202,33 +1332,51 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
     rd->n_live = live_cnt;
     rd->n_big = 0;
     // hub chunking pays off only when the round is too small to fill the GPU
-    rd->hub_on = (rd->big != nullptr && rd->items[T_SSSP] < rd->hub_max_items) ? 1u : 0u;
+    rd->hub_on =
+        (rd->big != nullptr && rd->items[T_SSSP] + rd->items[T_DP] + rd->items[T_HOP] < rd->hub_max_items) ? 1u : 0u;
   }
 }
 
 // ---------------------------------------------------------------------------
-// Light round kernel: warp tasks of types T_SPLIT .. T_SSSP.
+// Light round kernel: warp tasks of types T_SPLIT .. T_HOP (splits, seeds,
+// tour tables, extraction, distance items, DP states).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 3) k_light(const QDev* __restrict__ qd, RoundDesc* __restrict__ rd,
-                                               const uint32_t* __restrict__ pre, int nslots, GraphDev g) {
+#ifndef GSTB_LIGHT_MIN_BLOCKS
+#define GSTB_LIGHT_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(256, GSTB_LIGHT_MIN_BLOCKS) k_light(const QDev* __restrict__ qd, RoundDesc* __restrict__ rd,
+                                                  const uint32_t* __restrict__ pre, int nslots, GraphDev g) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t ntasks = __ldcg(&rd->light_tasks);
-  // the distance items' prefix over slots, staged once per block
-  __shared__ uint32_t s_pre[MAX_SLOTS + 1];
-  __shared__ RelaxHdr s_hdr[8][SSSP_W];
-  for (int i = threadIdx.x; i <= nslots; i += blockDim.x) s_pre[i] = __ldcg(pre + T_SSSP * (MAX_SLOTS + 1) + i);
+  // prefixes over slots of the item types with many items, staged once per block
+  __shared__ uint32_t s_pre[MAX_SLOTS + 1], s_dp[MAX_SLOTS + 1], s_hop[MAX_SLOTS + 1];
+  __shared__ RelaxHdr s_hdr[8][SSSP_WMAX];
+  for (int i = threadIdx.x; i <= nslots; i += blockDim.x) {
+    s_pre[i] = __ldcg(pre + T_SSSP * (MAX_SLOTS + 1) + i);
+    s_dp[i] = __ldcg(pre + T_DP * (MAX_SLOTS + 1) + i);
+    s_hop[i] = __ldcg(pre + T_HOP * (MAX_SLOTS + 1) + i);
+  }
   __syncthreads();
   SsspAcc acc;
   for (uint32_t task = warp; task < ntasks; task += nwarps) {
     int t = 0;
-    while (t < T_SSSP && task >= __ldcg(&rd->task_off[t + 1])) t++;
+    while (t < T_HOP && task >= __ldcg(&rd->task_off[t + 1])) t++;
     const uint32_t local = task - __ldcg(&rd->task_off[t]);
     const uint32_t* P = pre + t * (MAX_SLOTS + 1);
     const uint32_t total = __ldcg(&rd->items[t]);
     if (t == T_SSSP) {
-      sssp_task(qd, s_pre, nslots, total, local, g, lane, acc, rd, s_hdr[threadIdx.x >> 5]);
+      sssp_task(qd, s_pre, nslots, total, local, __ldcg(&rd->sssp_w), g, lane, acc, rd, s_hdr[threadIdx.x >> 5]);
+    } else if (t == T_DP || t == T_HOP) {
+      const uint32_t* S = t == T_DP ? s_dp : s_hop;
+      const uint32_t slot = find_slot_s(S, nslots, local);
+      const QDev& q = qd[slot];
+      const uint32_t st = q.qbuf[q.in_idx][local - S[slot]];
+      if (t == T_DP)
+        dp_item(q, g, st, lane, rd, slot);
+      else
+        hop_item(q, g, st, lane, rd, slot);
     } else if (t == T_TOUR) {
       tour_warp(qd[find_slot(P, nslots, local)], lane);
     } else if (t == T_EXTRACT) {
@@ -1251,49 +1399,36 @@ __global__ void __launch_bounds__(256, 3) k_light(const QDev* __restrict__ qd, R
   if (lane == 0) sssp_acc_flush(acc);
 }
 
-// Heavy round kernel: lower-bound table rows (one vertex per lane), then one
-// warp per DP state (unbounded, then hop-bounded).
+// Heavy round kernel: the arc chunks k_light handed over this round (hub
+// vertices of distance items, high-degree DP states), then lower-bound table
+// rows (8 lanes per vertex).
 __global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, const RoundDesc* __restrict__ rd,
                                                const uint32_t* __restrict__ pre, int nslots, GraphDev g) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  // hub arc chunks queued by k_light come first in the task space
   const uint32_t nbig = rd->big ? min(__ldcg(&rd->n_big), rd->big_cap) : 0u;
   const uint32_t ntasks = __ldcg(&rd->heavy_tasks) + nbig;
-  const uint32_t dp0 = __ldcg(&rd->task_off[T_DP]) + nbig, hop0 = __ldcg(&rd->task_off[T_HOP]) + nbig;
-  __shared__ uint32_t s_dp[MAX_SLOTS + 1], s_hop[MAX_SLOTS + 1], s_lb[MAX_SLOTS + 1];
+  __shared__ uint32_t s_lb[MAX_SLOTS + 1];
   __shared__ RelaxHdr s_hub[8];
-  for (int i = threadIdx.x; i <= nslots; i += blockDim.x) {
-    s_dp[i] = __ldcg(pre + T_DP * (MAX_SLOTS + 1) + i);
-    s_hop[i] = __ldcg(pre + T_HOP * (MAX_SLOTS + 1) + i);
-    s_lb[i] = __ldcg(pre + T_LB * (MAX_SLOTS + 1) + i);
-  }
+  for (int i = threadIdx.x; i <= nslots; i += blockDim.x) s_lb[i] = __ldcg(pre + T_LB * (MAX_SLOTS + 1) + i);
   __syncthreads();
+  const uint32_t n_lb = __ldcg(&rd->items[T_LB]);
   for (uint32_t task = warp; task < ntasks; task += nwarps) {
     if (task < nbig) {
-      hub_chunk(qd, __ldcg(rd->big + task), g, lane, &s_hub[threadIdx.x >> 5]);
+      const uint4 it = __ldcg(rd->big + task);
+      if (it.x & CH_GROW)
+        grow_chunk(qd, it, g, lane);
+      else
+        hub_chunk(qd, it, g, lane, &s_hub[threadIdx.x >> 5]);
       continue;
     }
-    if (task < dp0) {  // lower-bound table rows, 8 lanes per vertex
-      uint32_t it = (task - nbig) * 4u + (lane >> 3);
-      if (it < __ldcg(&rd->items[T_LB])) {
-        uint32_t slot = find_slot_s(s_lb, nslots, it);
-        const QDev& ql = qd[slot];
-        lbt_row8(ql, ql.lb_off + (it - s_lb[slot]), lane & 7u);
-      }
-      continue;
+    const uint32_t it = (task - nbig) * 4u + (lane >> 3);
+    if (it < n_lb) {
+      const uint32_t slot = find_slot_s(s_lb, nslots, it);
+      const QDev& ql = qd[slot];
+      lbt_row8(ql, ql.lb_off + (it - s_lb[slot]), lane & 7u);
     }
-    const bool hop = task >= hop0;
-    const uint32_t it = hop ? task - hop0 : task - dp0;
-    const uint32_t* P = hop ? s_hop : s_dp;
-    const uint32_t slot = find_slot_s(P, nslots, it);
-    const QDev& q = qd[slot];
-    const uint32_t s = q.qbuf[q.in_idx][it - P[slot]];
-    if (hop)
-      hop_item(q, g, s, lane);
-    else
-      dp_item(q, g, s, lane);
   }
 }
 
