@@ -82,22 +82,31 @@ enum {
   ST_SSSP_ENQ = 10,
 };
 
-// Written by kernels, read back by the host after every round.
-struct alignas(16) QCtl {
+// Written by kernels, read back by the host after every round.  The fields
+// sit in separate 32-byte sectors by access pattern: the incumbent is read by
+// every item, the list counters take one atomic per warp step, the statistics
+// are added once per warp and query, the rest is written once.
+struct alignas(64) QCtl {
+  // sector 0: the incumbent
+  uint32_t best;     // best feasible cost known (upper bound)
+  uint32_t root;
+  unsigned long long best_full;  // min over full states of cost << 32 | payload
+  uint32_t infeasible;  // the query groups are not connected
+  uint32_t pad0[3];
+  // sector 1: list append counters
   uint32_t n_near;   // append counter of the near-out list
   uint32_t n_far;    // append counter of the far list
   uint32_t n_far2;   // append counter of the far-out list (split rounds)
-  uint32_t best;     // best feasible cost known (upper bound)
   uint32_t overflow; // a list exceeded its capacity
+  uint32_t pad1[4];
+  // sectors 2-4: statistics
+  unsigned long long stat[12];
+  // sector 5: completion
   uint32_t n_edges;  // extraction: number of tree edges
   uint32_t status;   // extraction: 0 ok, 1 no solution, 2 cycle / inconsistency
-  uint32_t root;
-  unsigned long long best_full;  // min over full states of cost << 32 | payload
-  unsigned long long stat[12];
   uint32_t done;     // job finished (set by k_control)
   uint32_t final_status;  // gst_status of the finished job
-  uint32_t infeasible;    // the query groups are not connected
-  uint32_t pad;
+  uint32_t pad2[4];
 };
 
 // Per-query descriptor; the host rewrites it before each round.
@@ -157,6 +166,10 @@ __device__ __forceinline__ unsigned long long pack(uint32_t cost, uint32_t par) 
 }
 
 __device__ __forceinline__ uint32_t ld_cg(const uint32_t* p) { return __ldcg(p); }
+// The incumbent through L1: a value cached earlier in the same launch can be
+// higher than the current one, which only weakens pruning (every use of best
+// is an upper bound), and it spares the incumbent's L2 sector a read per item.
+__device__ __forceinline__ uint32_t ld_best(const QCtl* c) { return __ldca(&c->best); }
 __device__ __forceinline__ unsigned long long ld_cg(const unsigned long long* p) { return __ldcg(p); }
 
 // Software parallel-bit-deposit of the low bits of x into the set bits of mask.

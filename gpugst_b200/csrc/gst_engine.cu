@@ -45,8 +45,10 @@ using namespace gstb;
     }                                                     \
   } while (0)
 
-static cudaError_t& last_cuda_error() {
-  static thread_local cudaError_t e = cudaSuccess;
+// Last CUDA error met by any thread of the library (the serving loop runs on
+// its own thread), reported by gst_last_cuda_error.
+static std::atomic<cudaError_t>& last_cuda_error() {
+  static std::atomic<cudaError_t> e{cudaSuccess};
   return e;
 }
 
@@ -739,6 +741,8 @@ gst_status fill_result(Job* j, gst_result* r) {
 // C ABI
 // ---------------------------------------------------------------------------
 extern "C" {
+
+const char* gst_last_cuda_error(void) { return cudaGetErrorString(last_cuda_error().load()); }
 
 const char* gst_status_string(gst_status st) {
   switch (st) {

@@ -36,82 +36,98 @@ __device__ __forceinline__ uint32_t warp_sum(uint32_t x) {
   return x;
 }
 
-// ---------------------------------------------------------------------------
-// Warp-aggregated enqueue.  Every lane of the warp calls it (want may be
-// false).  A state is inserted into the near list when its cost is inside the
-// current window and into the far list otherwise; a 2-bit flag per state keeps
-// each list free of duplicates.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void enqueue_warp(bool want, uint32_t s, uint32_t cost, const QDev& q,
-                                             uint32_t* flags, uint32_t lane) {
-  bool nearq = cost < q.theta_hi;
-  bool take = false;
-  if (want) {
-    // near entries are flagged with the next round's parity; items of this
-    // round carry the other parity bit, which only their consumer clears
-    uint32_t bit = dflag_bit(s, nearq ? (q.par ^ 1u) : 2u);
-    uint32_t old = atomicOr(&flags[s >> 3], bit);
-    take = !(old & bit);
-  }
-  const unsigned FULL = 0xFFFFFFFFu;
+// Statistics of the query a warp is working for, kept in shared memory by
+// lane 0 and added to the query's counters only when the warp moves to
+// another query and at kernel end (one atomic per event would queue on the
+// query's control block).
+struct WarpStat {
+  QCtl* cur;
+  uint32_t v[12];
+};
+
+__device__ __forceinline__ void ws_init(WarpStat& w) {
+  w.cur = nullptr;
 #pragma unroll
-  for (int which = 0; which < 2; which++) {
-    bool mine = take && ((which == 0) == nearq);
-    unsigned m = __ballot_sync(FULL, mine);
-    if (m == 0) continue;
-    uint32_t leader = __ffs(m) - 1;
-    uint32_t base = 0;
-    if (lane == leader) {
-      uint32_t* cnt = which == 0 ? &q.ctl->n_near : &q.ctl->n_far;
-      base = atomicAdd(cnt, (uint32_t)__popc(m));
-    }
-    base = __shfl_sync(FULL, base, leader);
-    if (mine) {
-      uint32_t pos = base + __popc(m & ((1u << lane) - 1u));
-      uint32_t* buf = which == 0 ? q.qbuf[q.out_idx] : q.qbuf[q.far_idx];
-      if (pos < q.cap)
-        buf[pos] = s;
-      else
-        atomicExch(&q.ctl->overflow, 1u);
-    }
-  }
-  unsigned cntm = __popc(__ballot_sync(FULL, take));
-  if (lane == 0 && cntm) atomicAdd(&q.ctl->stat[ST_ENQ], (unsigned long long)cntm);
+  for (int i = 0; i < 12; i++) w.v[i] = 0u;
 }
 
-// Append for warps whose lanes may serve different queries (distance items
-// are processed by 8-lane groups).  The caller decides `take` (its pending
-// mask went from empty to non-empty); lanes are aggregated per (query, list)
-// with __match_any_sync.  `slot` identifies the query within the launch.
-__device__ __forceinline__ void append_multi(bool take, uint32_t item, bool nearq, const QDev& q,
-                                             uint32_t slot, uint32_t lane, uint32_t& enq) {
+__device__ __forceinline__ void ws_flush(WarpStat& w) {
+  if (w.cur)
+    for (int i = 0; i < 12; i++)
+      if (w.v[i]) atomicAdd(&w.cur->stat[i], (unsigned long long)w.v[i]);
+#pragma unroll
+  for (int i = 0; i < 12; i++) w.v[i] = 0u;
+}
+
+// Lane 0 only.
+__device__ __forceinline__ void ws_add(WarpStat& w, QCtl* c, int idx, uint32_t val) {
+  if (w.cur != c) {
+    ws_flush(w);
+    w.cur = c;
+  }
+  w.v[idx] += val;
+}
+
+// Warp-local staging of list appends.  The near-out and far entries of one
+// query collect in shared memory and reach the global lists in bulk: every
+// warp working for a query appends to the same two counters, and one counter
+// atomic per flush instead of one per warp step keeps them from queueing.
+constexpr uint32_t WBUF = 256;
+struct WarpBuf {
+  const QDev* q;
+  uint32_t nN, nF;
+  uint32_t itN[WBUF], itF[WBUF];
+};
+
+__device__ __forceinline__ void wb_init(WarpBuf& b) {  // lane 0
+  b.q = nullptr;
+  b.nN = b.nF = 0u;
+}
+
+// Every lane of the warp calls it.
+__device__ __forceinline__ void wb_flush(WarpBuf& b, uint32_t lane) {
   const unsigned FULL = 0xFFFFFFFFu;
-  uint32_t key = take ? (slot * 2u + (nearq ? 0u : 1u)) : 0xFFFFFFFFu;
-  unsigned m = __match_any_sync(FULL, key);
-  uint32_t leader = __ffs(m) - 1;
-  uint32_t base = 0;
-  if (take && lane == leader) {
-    uint32_t* cnt = nearq ? &q.ctl->n_near : &q.ctl->n_far;
-    base = atomicAdd(cnt, (uint32_t)__popc(m));
+  __syncwarp();
+  const QDev* q = b.q;
+  const uint32_t nN = b.nN, nF = b.nF;
+  if (q != nullptr && (nN | nF) != 0u) {
+    uint32_t bN = 0, bF = 0;
+    if (lane == 0) {
+      if (nN) bN = atomicAdd(&q->ctl->n_near, nN);
+      if (nF) bF = atomicAdd(&q->ctl->n_far, nF);
+    }
+    bN = __shfl_sync(FULL, bN, 0);
+    bF = __shfl_sync(FULL, bF, 0);
+    uint32_t* outN = q->qbuf[q->out_idx];
+    uint32_t* outF = q->qbuf[q->far_idx];
+    const uint32_t cap = q->cap;
+    bool ovf = false;
+    for (uint32_t i = lane; i < nN; i += 32u) {
+      if (bN + i < cap)
+        outN[bN + i] = b.itN[i];
+      else
+        ovf = true;
+    }
+    for (uint32_t i = lane; i < nF; i += 32u) {
+      if (bF + i < cap)
+        outF[bF + i] = b.itF[i];
+      else
+        ovf = true;
+    }
+    if (__any_sync(FULL, ovf) && lane == 0) atomicExch(&q->ctl->overflow, 1u);
   }
-  base = __shfl_sync(FULL, base, leader);
-  if (take) {
-    uint32_t pos = base + __popc(m & ((1u << lane) - 1u));
-    uint32_t* buf = nearq ? q.qbuf[q.out_idx] : q.qbuf[q.far_idx];
-    if (pos < q.cap)
-      buf[pos] = item;
-    else
-      atomicExch(&q.ctl->overflow, 1u);
-    enq++;
-  }
+  __syncwarp();
+  if (lane == 0) b.nN = b.nF = 0u;
+  __syncwarp();
 }
 
-// Warp-wide append of up to U items per lane to the near-out and far lists
-// of one query: one reservation per list and warp, then plain stores.  Every
-// lane of the warp calls it; returns this lane's number of appended items.
+// Append up to U items per lane to the near-out and far lists of query q
+// through the warp's buffer.  Every lane of the warp calls it; returns this
+// lane's number of appended items.
 template <int U>
 __device__ __forceinline__ uint32_t append_lists(const bool (&takeN)[U], const bool (&takeF)[U],
-                                                 const uint32_t (&item)[U], const QDev& q, uint32_t lane) {
+                                                 const uint32_t (&item)[U], const QDev& q, uint32_t lane,
+                                                 WarpBuf& b) {
   const unsigned FULL = 0xFFFFFFFFu;
   uint32_t cN = 0, cF = 0;
 #pragma unroll
@@ -130,34 +146,66 @@ __device__ __forceinline__ uint32_t append_lists(const bool (&takeN)[U], const b
     }
   }
   const uint32_t totN = __shfl_sync(FULL, xN, 31), totF = __shfl_sync(FULL, xF, 31);
-  uint32_t bN = 0, bF = 0;
-  if (lane == 0) {
-    if (totN) bN = atomicAdd(&q.ctl->n_near, totN);
-    if (totF) bF = atomicAdd(&q.ctl->n_far, totF);
+  __syncwarp();
+  if (b.q != &q || b.nN + totN > WBUF || b.nF + totF > WBUF) {
+    wb_flush(b, lane);
+    if (lane == 0) b.q = &q;
+    __syncwarp();
   }
-  uint32_t pN = __shfl_sync(FULL, bN, 0) + xN - cN, pF = __shfl_sync(FULL, bF, 0) + xF - cF;
-  uint32_t* outN = q.qbuf[q.out_idx];
-  uint32_t* outF = q.qbuf[q.far_idx];
-  bool ovf = false;
+  const uint32_t oN = b.nN, oF = b.nF;
+  uint32_t pN = oN + xN - cN, pF = oF + xF - cF;
 #pragma unroll
   for (int u = 0; u < U; u++) {
-    if (takeN[u]) {
-      if (pN < q.cap)
-        outN[pN] = item[u];
-      else
-        ovf = true;
-      pN++;
-    }
-    if (takeF[u]) {
-      if (pF < q.cap)
-        outF[pF] = item[u];
-      else
-        ovf = true;
-      pF++;
-    }
+    if (takeN[u]) b.itN[pN++] = item[u];
+    if (takeF[u]) b.itF[pF++] = item[u];
   }
-  if (ovf) atomicExch(&q.ctl->overflow, 1u);
+  __syncwarp();
+  if (lane == 0) {
+    b.nN = oN + totN;
+    b.nF = oF + totF;
+  }
+  __syncwarp();
   return cN + cF;
+}
+
+// Enqueue of DP state s at `cost`: the near list when the cost is inside the
+// current window, the far list otherwise; a flag bit per state and list
+// keeps each list free of duplicates (near entries carry the next round's
+// parity).  Every lane calls it (want may be false); returns 1 if this lane
+// enqueued.
+__device__ __forceinline__ uint32_t enqueue_warp(bool want, uint32_t s, uint32_t cost, const QDev& q, uint32_t lane,
+                                                 WarpBuf& b) {
+  const bool nearq = cost < q.theta_hi;
+  bool take = false;
+  if (want) {
+    const uint32_t bit = dflag_bit(s, nearq ? (q.par ^ 1u) : 2u);
+    take = !(atomicOr(&q.dflag[s >> 3], bit) & bit);
+  }
+  const bool tN[1] = {take && nearq}, tF[1] = {take && !nearq};
+  const uint32_t it[1] = {s};
+  return append_lists<1>(tN, tF, it, q, lane, b);
+}
+
+// Single-entry push for warps whose lanes may serve different queries
+// (split and seed tasks): lanes are aggregated per (query, list) with
+// __match_any_sync.  which: 0 = near-out list, 1 = far-out list.
+__device__ __forceinline__ void push_multi(bool take, uint32_t item, uint32_t which, const QDev& q, uint32_t slot,
+                                           uint32_t lane) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  const uint32_t key = take ? slot * 2u + which : 0xFFFFFFFFu;
+  const unsigned m = __match_any_sync(FULL, key);
+  const uint32_t leader = (uint32_t)(__ffs(m) - 1);
+  uint32_t base = 0;
+  if (take && lane == leader) base = atomicAdd(which == 0u ? &q.ctl->n_near : &q.ctl->n_far2, (uint32_t)__popc(m));
+  base = __shfl_sync(FULL, base, leader);
+  if (take) {
+    const uint32_t pos = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+    uint32_t* buf = which == 0u ? q.qbuf[q.out_idx] : q.qbuf[q.far2_idx];
+    if (pos < q.cap)
+      buf[pos] = item;
+    else
+      atomicExch(&q.ctl->overflow, 1u);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -180,7 +228,7 @@ struct GrowCnt {
 
 __device__ __forceinline__ void grow_arcs(const QDev& q, const GraphDev& g, uint32_t lane, uint32_t v, uint32_t p,
                                           uint32_t comp, uint32_t c, uint32_t best, uint32_t lim, int dnext,
-                                          uint32_t a0, uint32_t a1, GrowCnt& cnt) {
+                                          uint32_t a0, uint32_t a1, GrowCnt& cnt, WarpBuf& wb) {
   const int k = q.k;
   const uint32_t nd = (uint32_t)q.nd, thi = q.theta_hi, par = q.par;
   const unsigned short* __restrict__ lbt = q.lbt;
@@ -231,7 +279,7 @@ __device__ __forceinline__ void grow_arcs(const QDev& q, const GraphDev& g, uint
       tN[u] = take && nc[u] < thi;
       tF[u] = take && !(nc[u] < thi);
     }
-    cnt.enq += append_lists<GROW_U>(tN, tF, t, q, lane);
+    cnt.enq += append_lists<GROW_U>(tN, tF, t, q, lane, wb);
   }
 }
 
@@ -280,7 +328,7 @@ __device__ __forceinline__ void load_dl(const QDev& q, uint32_t v, uint32_t (&dl
 // Unbounded DP item (v, p).
 // ---------------------------------------------------------------------------
 __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t lane, RoundDesc* __restrict__ rd,
-                        uint32_t slot) {
+                        uint32_t slot, WarpStat& ws, WarpBuf& wb) {
   const unsigned FULL = 0xFFFFFFFFu;
   const int k = q.k;
   const uint32_t K2 = 1u << k, full = (uint32_t)q.full;
@@ -288,11 +336,11 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
   if (lane == 0) atomicAnd(&q.dflag[s >> 3], ~dflag_bit(s, q.par));
   __syncwarp();
   uint32_t c = __shfl_sync(FULL, (uint32_t)(ld_cg(q.table + s) >> 32), 0);
-  uint32_t best = __shfl_sync(FULL, ld_cg(&q.ctl->best), 0);
+  uint32_t best = __shfl_sync(FULL, ld_best(q.ctl), 0);
   if (c == INF32 || c > best) return;
   unsigned long long* row = q.table + (size_t)v * K2;
   if (p == full) {
-    if (lane == 0) atomicMin(&q.ctl->best, c);
+    if (lane == 0 && c < best) atomicMin(&q.ctl->best, c);
     return;
   }
   const uint32_t comp = full ^ p;
@@ -300,26 +348,33 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
   unsigned long long raw_sum;
   load_dl(q, v, dl, sum_ok, comp, raw_sum);
   if (lane == 0) {
-    // complement merge straight into the full state (DPQ.cu:82-94)
+    // complement merge straight into the full state (DPQ.cu:82-94); a full
+    // state of cost equal to best is still recorded: best may come from a
+    // bound-only tree (star or one-label) that has no table entry
     uint32_t cc = (uint32_t)(ld_cg(row + comp) >> 32);
     if (cc != INF32) {
       unsigned long long m = (unsigned long long)c + cc;
-      if (m < INF32) {
+      if (m <= best) {
         atomicMin(row + full, pack((uint32_t)m, PAR_MERGE | p));
-        atomicMin(&q.ctl->best, (uint32_t)m);
         atomicMin(&q.ctl->best_full, (m << 32) | v);
+        if (m < best) {
+          atomicMin(&q.ctl->best, (uint32_t)m);
+          best = (uint32_t)m;
+        }
       }
     }
     // one-label completion: T(v,p) plus shortest paths to the missing groups
     // (DPQ.cu:95-107, CPUNONHOP.h:684-699)
     if (sum_ok) {
       unsigned long long ol = (unsigned long long)c + raw_sum;
-      if (ol < INF32) atomicMin(&q.ctl->best, (uint32_t)ol);
+      if (ol < best) {
+        atomicMin(&q.ctl->best, (uint32_t)ol);
+        best = (uint32_t)ol;
+      }
     }
-    atomicAdd(&q.ctl->stat[ST_EXPANDED], 1ull);
+    ws_add(ws, q.ctl, ST_EXPANDED, 1u);
   }
-  __syncwarp();
-  best = __shfl_sync(FULL, ld_cg(&q.ctl->best), 0);
+  best = __shfl_sync(FULL, best, 0);
   const unsigned short* lbt = q.lbt;
   uint32_t lbv = __ldg(lbt + ((size_t)v << k) + comp);
   if ((unsigned long long)c + lbv > best) return;
@@ -335,18 +390,13 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
     if (rd->hub_on && a1 - a0 >= rd->hub_min_deg &&
         push_grow_chunks(rd, slot, false, s, a0 + GROW_LOCAL, a1, lane))
       a1 = a0 + GROW_LOCAL;
-    grow_arcs(q, g, lane, v, p, comp, c, best, lim, -1, a0, a1, gc);
-  }
-  uint32_t scanned = gc.arcs, upd = gc.upd;
-  {
-    const uint32_t e = warp_sum(gc.enq);
-    if (lane == 0 && e) atomicAdd(&q.ctl->stat[ST_ENQ], (unsigned long long)e);
+    grow_arcs(q, g, lane, v, p, comp, c, best, lim, -1, a0, a1, gc, wb);
   }
   // merge with every proper, non-empty subset p2 of the complement
   // (DPQ.cu:140-170; the complement itself went to the full state above)
+  uint32_t merges = 0;
   {
     const uint32_t nsub = (1u << __popc(comp)) - 2u;
-    uint32_t merges = 0;
     for (uint32_t b = 0; b < nsub; b += 32) {
       uint32_t idx = b + lane;
       bool want = false;
@@ -367,25 +417,20 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
               t = (v << k) | qset;
               atomicMin(q.table + t, pack(m32, PAR_MERGE | p));
               want = true;
-              upd++;
+              gc.upd++;
             }
           }
         }
       }
-      enqueue_warp(want, t, m32, q, q.dflag, lane);
+      gc.enq += enqueue_warp(want, t, m32, q, lane, wb);
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) merges += __shfl_xor_sync(FULL, merges, o);
-    if (lane == 0 && merges) atomicAdd(&q.ctl->stat[ST_MERGES], (unsigned long long)merges);
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    scanned += __shfl_xor_sync(FULL, scanned, o);
-    upd += __shfl_xor_sync(FULL, upd, o);
-  }
+  const uint32_t sa = warp_sum(gc.arcs), su = warp_sum(gc.upd), se = warp_sum(gc.enq), sm = warp_sum(merges);
   if (lane == 0) {
-    atomicAdd(&q.ctl->stat[ST_ARCS], (unsigned long long)scanned);
-    atomicAdd(&q.ctl->stat[ST_UPDATES], (unsigned long long)upd);
+    ws_add(ws, q.ctl, ST_ARCS, sa);
+    ws_add(ws, q.ctl, ST_UPDATES, su);
+    ws_add(ws, q.ctl, ST_ENQ, se);
+    ws_add(ws, q.ctl, ST_MERGES, sm);
   }
 }
 
@@ -393,7 +438,7 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
 // Hop-bounded DP item (v, p, d): state id ((v << k) | p) * nd + d.
 // ---------------------------------------------------------------------------
 __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t lane, RoundDesc* __restrict__ rd,
-                         uint32_t slot) {
+                         uint32_t slot, WarpStat& ws, WarpBuf& wb) {
   const unsigned FULL = 0xFFFFFFFFu;
   const int k = q.k, nd = q.nd, D = q.D;
   const uint32_t K2 = 1u << k, full = (uint32_t)q.full;
@@ -402,7 +447,7 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
   if (lane == 0) atomicAnd(&q.dflag[s >> 3], ~dflag_bit(s, q.par));
   __syncwarp();
   uint32_t c = __shfl_sync(FULL, (uint32_t)(ld_cg(q.table + s) >> 32), 0);
-  uint32_t best = __shfl_sync(FULL, ld_cg(&q.ctl->best), 0);
+  uint32_t best = __shfl_sync(FULL, ld_best(q.ctl), 0);
   if (c == INF32 || c > best) return;
   // dominance: the same subset at a smaller hop count and no higher cost
   {
@@ -411,11 +456,11 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
     if (__any_sync(FULL, dom)) return;
   }
   if (p == full) {
-    if (lane == 0) atomicMin(&q.ctl->best, c);
+    if (lane == 0 && c < best) atomicMin(&q.ctl->best, c);
     return;
   }
   const uint32_t comp = full ^ p;
-  if (lane == 0) atomicAdd(&q.ctl->stat[ST_EXPANDED], 1ull);
+  if (lane == 0) ws_add(ws, q.ctl, ST_EXPANDED, 1u);
   const unsigned short* lbt = q.lbt;
   uint32_t lbv = __ldg(lbt + ((size_t)v << k) + comp);
   if ((unsigned long long)c + lbv > best) return;
@@ -427,21 +472,16 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
     if (rd->hub_on && a1 - a0 >= rd->hub_min_deg &&
         push_grow_chunks(rd, slot, true, s, a0 + GROW_LOCAL, a1, lane))
       a1 = a0 + GROW_LOCAL;
-    grow_arcs(q, g, lane, v, p, comp, c, best, lim, (int)d + 1, a0, a1, gc);
-  }
-  uint32_t scanned = gc.arcs, upd = gc.upd;
-  {
-    const uint32_t e = warp_sum(gc.enq);
-    if (lane == 0 && e) atomicAdd(&q.ctl->stat[ST_ENQ], (unsigned long long)e);
+    grow_arcs(q, g, lane, v, p, comp, c, best, lim, (int)d + 1, a0, a1, gc, wb);
   }
   // merge with (v, p2, d2), p2 a non-empty subset of the complement,
   // d2 <= D - d, into (v, p|p2, max(d, d2))  (CPUHOP.h:208-227)
+  uint32_t merges = 0;
   {
     const uint32_t nsub = (1u << __popc(comp)) - 1u;
     const uint32_t nd2 = (uint32_t)D - d + 1u;
     const uint32_t npairs = nsub * nd2;
     unsigned long long* rowv = q.table + ((size_t)v << k) * nd;
-    uint32_t merges = 0;
     for (uint32_t b = 0; b < npairs; b += 32) {
       uint32_t idx = b + lane;
       bool want = false;
@@ -456,38 +496,35 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
           uint32_t qset = p | p2;
           uint32_t ndd = max(d, d2);
           uint32_t par = PAR_MERGE | p | (d << 8) | (d2 << 11);
-          if (m < INF32) {
+          if (m <= best) {
             m32 = (uint32_t)m;
             t = ((v << k) | qset) * (uint32_t)nd + ndd;
             if (qset == full) {
+              // recorded at cost == best too: best may come from a tree
+              // that has no table entry
               atomicMin(q.table + t, pack(m32, par));
-              atomicMin(&q.ctl->best, m32);
               atomicMin(&q.ctl->best_full, ((unsigned long long)m32 << 32) | (v * 8u + ndd));
+              if (m32 < best) atomicMin(&q.ctl->best, m32);
             } else {
               uint32_t lbq = __ldg(lbt + ((size_t)v << k) + (full ^ qset));
               if (m + lbq <= best && m32 < (uint32_t)(ld_cg(q.table + t) >> 32)) {
                 atomicMin(q.table + t, pack(m32, par));
                 want = true;
-                upd++;
+                gc.upd++;
               }
             }
           }
         }
       }
-      enqueue_warp(want, t, m32, q, q.dflag, lane);
+      gc.enq += enqueue_warp(want, t, m32, q, lane, wb);
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) merges += __shfl_xor_sync(FULL, merges, o);
-    if (lane == 0 && merges) atomicAdd(&q.ctl->stat[ST_MERGES], (unsigned long long)merges);
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    scanned += __shfl_xor_sync(FULL, scanned, o);
-    upd += __shfl_xor_sync(FULL, upd, o);
-  }
+  const uint32_t sa = warp_sum(gc.arcs), su = warp_sum(gc.upd), se = warp_sum(gc.enq), sm = warp_sum(merges);
   if (lane == 0) {
-    atomicAdd(&q.ctl->stat[ST_ARCS], (unsigned long long)scanned);
-    atomicAdd(&q.ctl->stat[ST_UPDATES], (unsigned long long)upd);
+    ws_add(ws, q.ctl, ST_ARCS, sa);
+    ws_add(ws, q.ctl, ST_UPDATES, su);
+    ws_add(ws, q.ctl, ST_ENQ, se);
+    ws_add(ws, q.ctl, ST_MERGES, sm);
   }
 }
 
@@ -546,23 +583,6 @@ struct RelaxCnt {
   uint32_t arcs = 0, upd = 0, enq = 0;
 };
 
-// Per-warp statistics of one query, flushed when the warp moves to another
-// query and at kernel end (held by lane 0).
-struct SsspAcc {
-  QCtl* cur = nullptr;
-  uint32_t items = 0, arcs = 0, upd = 0, enq = 0;
-};
-
-__device__ __forceinline__ void sssp_acc_flush(SsspAcc& a) {
-  if (a.cur) {
-    if (a.items) atomicAdd(&a.cur->stat[ST_SSSP], (unsigned long long)a.items);
-    if (a.arcs) atomicAdd(&a.cur->stat[ST_SSSP_ARCS], (unsigned long long)a.arcs);
-    if (a.upd) atomicAdd(&a.cur->stat[ST_SSSP_UPDATES], (unsigned long long)a.upd);
-    if (a.enq) atomicAdd(&a.cur->stat[ST_SSSP_ENQ], (unsigned long long)a.enq);
-  }
-  a.items = a.arcs = a.upd = a.enq = 0;
-}
-
 __device__ __forceinline__ uint32_t sel8(const uint4& a, const uint4& b, uint32_t i) {
   const uint4& h = i < 4u ? a : b;
   const uint32_t j = i & 3u;
@@ -578,7 +598,7 @@ __device__ __forceinline__ uint32_t sel8(const uint4& a, const uint4& b, uint32_
 // aggregated over the whole warp.
 __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __restrict__ h, uint32_t x, uint32_t i0,
                                            uint32_t i1, uint32_t capb, const GraphDev& g, uint32_t lane,
-                                           RelaxCnt& cnt) {
+                                           RelaxCnt& cnt, WarpBuf& wb) {
   const unsigned FULL = 0xFFFFFFFFu;
   const uint32_t lo_end = __shfl_sync(FULL, x, i0 == 0u ? 0u : i0 - 1u);
   const uint32_t f0 = i0 == 0u ? 0u : lo_end;
@@ -661,23 +681,24 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
       tN[u] = oN[u] == 0u;
       tF[u] = oF[u] == 0u;
     }
-    cnt.enq += append_lists<SSSP_U>(tN, tF, itv, q, lane);
+    cnt.enq += append_lists<SSSP_U>(tN, tF, itv, q, lane, wb);
   }
 }
 
-__device__ __forceinline__ void relax_cnt_flush(QCtl* c, RelaxCnt cnt, uint32_t items, uint32_t lane) {
+// Warp-reduce a relaxation's counters into the warp's statistics.
+__device__ __forceinline__ void relax_cnt_add(WarpStat& ws, QCtl* c, RelaxCnt cnt, uint32_t items, uint32_t lane) {
   const uint32_t a = warp_sum(cnt.arcs), u = warp_sum(cnt.upd), e = warp_sum(cnt.enq);
   if (lane == 0) {
-    if (items) atomicAdd(&c->stat[ST_SSSP], (unsigned long long)items);
-    if (a) atomicAdd(&c->stat[ST_SSSP_ARCS], (unsigned long long)a);
-    if (u) atomicAdd(&c->stat[ST_SSSP_UPDATES], (unsigned long long)u);
-    if (e) atomicAdd(&c->stat[ST_SSSP_ENQ], (unsigned long long)e);
+    ws_add(ws, c, ST_SSSP, items);
+    ws_add(ws, c, ST_SSSP_ARCS, a);
+    ws_add(ws, c, ST_SSSP_UPDATES, u);
+    ws_add(ws, c, ST_SSSP_ENQ, e);
   }
 }
 
 __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restrict__ pre, int nslots,
-                          uint32_t total, uint32_t task, uint32_t W, const GraphDev& g, uint32_t lane, SsspAcc& acc,
-                          RoundDesc* __restrict__ rd, RelaxHdr* __restrict__ sh) {
+                          uint32_t total, uint32_t task, uint32_t W, const GraphDev& g, uint32_t lane, WarpStat& ws,
+                          RoundDesc* __restrict__ rd, RelaxHdr* __restrict__ sh, WarpBuf& wb) {
   const unsigned FULL = 0xFFFFFFFFu;
   const uint32_t it = task * W + lane;
   const bool valid = lane < W && it < total;
@@ -693,7 +714,7 @@ __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restric
     const uint32_t m = atomicExch(&q.sflag[(size_t)q.par * V + v], 0u);
     const uint4* drow = reinterpret_cast<const uint4*>(q.dist + (size_t)v * 8);
     const uint4 da = __ldcg(drow), db = __ldcg(drow + 1);
-    uint32_t best = ld_cg(&q.ctl->best);
+    uint32_t best = ld_best(q.ctl);
     const uint32_t b0 = __ldg(g.beg + v), b1 = __ldg(g.beg + v + 1);
     uint4 wa = make_uint4(b1, b1, b1, b1), wb = wa;
     if (g.wcut != nullptr) {
@@ -787,25 +808,15 @@ __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restric
     const uint32_t n_items = __popc(amask & rmask);
     const QDev& q = qd[si];
     RelaxCnt cnt;
-    relax_flat(q, sh, x, i0, i1, cb, g, lane, cnt);
-    const uint32_t a = warp_sum(cnt.arcs), u = warp_sum(cnt.upd), e = warp_sum(cnt.enq);
-    if (lane == 0) {
-      if (acc.cur != q.ctl) {
-        sssp_acc_flush(acc);
-        acc.cur = q.ctl;
-      }
-      acc.items += n_items;
-      acc.arcs += a;
-      acc.upd += u;
-      acc.enq += e;
-    }
+    relax_flat(q, sh, x, i0, i1, cb, g, lane, cnt, wb);
+    relax_cnt_add(ws, q.ctl, cnt, n_items, lane);
   }
 }
 
 // One hub chunk (k_heavy, one warp): relax arcs [first, end) of vertex v for
 // the pending groups recorded by k_light.  Same relaxation as sssp_task.
 __device__ void hub_chunk(const QDev* __restrict__ qd, const uint4 item, const GraphDev& g, uint32_t lane,
-                          RelaxHdr* __restrict__ sh) {
+                          RelaxHdr* __restrict__ sh, WarpStat& ws, WarpBuf& wb) {
   const unsigned FULL = 0xFFFFFFFFu;
   if (item.z >= item.w) return;  // filler entry of a chunk run that did not fit
   const uint32_t slot = item.x & 0xFFFFu, v = item.y;
@@ -814,7 +825,7 @@ __device__ void hub_chunk(const QDev* __restrict__ qd, const uint4 item, const G
   if (lane == 0) {
     const uint4* drow = reinterpret_cast<const uint4*>(q.dist + (size_t)v * 8);
     const uint4 da = __ldcg(drow), db = __ldcg(drow + 1);
-    const uint32_t best = ld_cg(&q.ctl->best);
+    const uint32_t best = ld_best(q.ctl);
     const uint32_t d[8] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z, db.w};
     capb = (uint32_t)((unsigned long long)best * q.cap_num / q.cap_den);
     uint32_t rm = 0, dmin = INF32;
@@ -839,15 +850,16 @@ __device__ void hub_chunk(const QDev* __restrict__ qd, const uint4 item, const G
   n = __shfl_sync(FULL, n, 0);
   if (n == 0) return;
   RelaxCnt cnt;
-  relax_flat(q, sh, n, 0u, 1u, capb, g, lane, cnt);  // one item: every lane holds its prefix n
-  relax_cnt_flush(q.ctl, cnt, 0u, lane);
+  relax_flat(q, sh, n, 0u, 1u, capb, g, lane, cnt, wb);  // one item: every lane holds its prefix n
+  relax_cnt_add(ws, q.ctl, cnt, 0u, lane);
 }
 
 // One DP grow chunk (k_heavy, one warp): arcs [first, end) of a state that a
 // k_light warp handed over.  The state's current cost is read again (it can
 // only have dropped, and a lower cost grows validly too) and the gates of the
 // state's own expansion are re-checked.
-__device__ void grow_chunk(const QDev* __restrict__ qd, const uint4 item, const GraphDev& g, uint32_t lane) {
+__device__ void grow_chunk(const QDev* __restrict__ qd, const uint4 item, const GraphDev& g, uint32_t lane,
+                           WarpStat& ws, WarpBuf& wb) {
   const unsigned FULL = 0xFFFFFFFFu;
   if (item.z >= item.w) return;  // filler entry of a chunk run that did not fit
   const uint32_t slot = item.x & 0xFFFFu;
@@ -860,7 +872,7 @@ __device__ void grow_chunk(const QDev* __restrict__ qd, const uint4 item, const 
   uint32_t c = 0, best = 0, lbv = 0;
   if (lane == 0) {
     c = (uint32_t)(ld_cg(q.table + s) >> 32);
-    best = ld_cg(&q.ctl->best);
+    best = ld_best(q.ctl);
     lbv = __ldg(q.lbt + ((size_t)v << k) + comp);
   }
   c = __shfl_sync(FULL, c, 0);
@@ -869,12 +881,12 @@ __device__ void grow_chunk(const QDev* __restrict__ qd, const uint4 item, const 
   if (c == INF32 || c > best || (unsigned long long)c + lbv > best) return;
   if (!hop && 2ull * c > best) return;
   GrowCnt gc;
-  grow_arcs(q, g, lane, v, p, comp, c, best, best - c, hop ? (int)d + 1 : -1, item.z, item.w, gc);
+  grow_arcs(q, g, lane, v, p, comp, c, best, best - c, hop ? (int)d + 1 : -1, item.z, item.w, gc, wb);
   const uint32_t a = warp_sum(gc.arcs), u = warp_sum(gc.upd), e = warp_sum(gc.enq);
   if (lane == 0) {
-    if (a) atomicAdd(&q.ctl->stat[ST_ARCS], (unsigned long long)a);
-    if (u) atomicAdd(&q.ctl->stat[ST_UPDATES], (unsigned long long)u);
-    if (e) atomicAdd(&q.ctl->stat[ST_ENQ], (unsigned long long)e);
+    ws_add(ws, q.ctl, ST_ARCS, a);
+    ws_add(ws, q.ctl, ST_UPDATES, u);
+    ws_add(ws, q.ctl, ST_ENQ, e);
   }
 }
 
@@ -883,16 +895,11 @@ __device__ void grow_chunk(const QDev* __restrict__ qd, const uint4 item, const 
 // (every new cost is >= the cost of the item that produced it) -> dropped.
 // Distance items are vertices with a mask of pending groups; DP items are
 // states.  Items moved to the near list carry the parity of the next round.
-__device__ __forceinline__ void push_list(const QDev& q, uint32_t* cnt, uint32_t* buf, uint32_t item) {
-  uint32_t pos = atomicAdd(cnt, 1u);
-  if (pos < q.cap)
-    buf[pos] = item;
-  else
-    atomicExch(&q.ctl->overflow, 1u);
-}
-
-__device__ void split_item(const QDev& q, uint32_t s) {
+// The caller pushes `s` to the near-out list if toN and to the far-out list
+// if toF (push_multi, warp-aggregated).
+__device__ void split_item(const QDev& q, uint32_t s, bool& toN, bool& toF) {
   uint32_t best = ld_cg(&q.ctl->best);
+  toN = toF = false;
   if (q.phase == PH_SSSP) {
     const uint32_t V = q.nv;
     const uint32_t capb = (uint32_t)((unsigned long long)best * q.cap_num / q.cap_den);
@@ -907,8 +914,8 @@ __device__ void split_item(const QDev& q, uint32_t s) {
       else
         kb |= 1u << t;
     }
-    if (nb && atomicOr(&q.sflag[(size_t)q.par * V + s], nb) == 0u) push_list(q, &q.ctl->n_near, q.qbuf[q.out_idx], s);
-    if (kb && atomicOr(&q.sflag[(size_t)2 * V + s], kb) == 0u) push_list(q, &q.ctl->n_far2, q.qbuf[q.far2_idx], s);
+    toN = nb && atomicOr(&q.sflag[(size_t)q.par * V + s], nb) == 0u;
+    toF = kb && atomicOr(&q.sflag[(size_t)2 * V + s], kb) == 0u;
     return;
   }
   uint32_t cost = (uint32_t)(ld_cg(q.table + s) >> 32);
@@ -918,17 +925,27 @@ __device__ void split_item(const QDev& q, uint32_t s) {
     atomicAnd(&q.dflag[s >> 3], ~dflag_bit(s, 2u));
     uint32_t bit = dflag_bit(s, q.par);
     uint32_t old = atomicOr(&q.dflag[s >> 3], bit);
-    if (!(old & bit)) push_list(q, &q.ctl->n_near, q.qbuf[q.out_idx], s);
+    toN = !(old & bit);
   } else {
-    push_list(q, &q.ctl->n_far2, q.qbuf[q.far2_idx], s);
+    toF = true;
   }
 }
 
-// Member item v*8+j -> distance 0; the vertex enters the first near list.
-__device__ void sseed_item(const QDev& q, uint32_t item) {
+// Member item v*8+j -> distance 0; the vertex enters the first near list
+// (the caller pushes v if toN).
+__device__ void sseed_item(const QDev& q, uint32_t item, bool& toN) {
   uint32_t v = item >> 3, j = item & 7u;
   q.dist[item] = 0;
-  if (atomicOr(&q.sflag[(size_t)q.par * q.nv + v], 1u << j) == 0u) push_list(q, &q.ctl->n_near, q.qbuf[q.out_idx], v);
+  toN = atomicOr(&q.sflag[(size_t)q.par * q.nv + v], 1u << j) == 0u;
+}
+
+// Single append (DP seeding only: once per member state of a query).
+__device__ __forceinline__ void push_list(const QDev& q, uint32_t* cnt, uint32_t* buf, uint32_t item) {
+  uint32_t pos = atomicAdd(cnt, 1u);
+  if (pos < q.cap)
+    buf[pos] = item;
+  else
+    atomicExch(&q.ctl->overflow, 1u);
 }
 
 // Cost-0 states: every non-empty subset of a member's mask (DPQ.cu:341-358).
@@ -1353,13 +1370,20 @@ __global__ void __launch_bounds__(256, GSTB_LIGHT_MIN_BLOCKS) k_light(const QDev
   // prefixes over slots of the item types with many items, staged once per block
   __shared__ uint32_t s_pre[MAX_SLOTS + 1], s_dp[MAX_SLOTS + 1], s_hop[MAX_SLOTS + 1];
   __shared__ RelaxHdr s_hdr[8][SSSP_WMAX];
+  __shared__ WarpStat s_ws[8];
+  __shared__ WarpBuf s_wb[8];
+  WarpStat& ws = s_ws[threadIdx.x >> 5];
+  WarpBuf& wb = s_wb[threadIdx.x >> 5];
+  if (lane == 0) {
+    ws_init(ws);
+    wb_init(wb);
+  }
   for (int i = threadIdx.x; i <= nslots; i += blockDim.x) {
     s_pre[i] = __ldcg(pre + T_SSSP * (MAX_SLOTS + 1) + i);
     s_dp[i] = __ldcg(pre + T_DP * (MAX_SLOTS + 1) + i);
     s_hop[i] = __ldcg(pre + T_HOP * (MAX_SLOTS + 1) + i);
   }
   __syncthreads();
-  SsspAcc acc;
   for (uint32_t task = warp; task < ntasks; task += nwarps) {
     int t = 0;
     while (t < T_HOP && task >= __ldcg(&rd->task_off[t + 1])) t++;
@@ -1367,36 +1391,45 @@ __global__ void __launch_bounds__(256, GSTB_LIGHT_MIN_BLOCKS) k_light(const QDev
     const uint32_t* P = pre + t * (MAX_SLOTS + 1);
     const uint32_t total = __ldcg(&rd->items[t]);
     if (t == T_SSSP) {
-      sssp_task(qd, s_pre, nslots, total, local, __ldcg(&rd->sssp_w), g, lane, acc, rd, s_hdr[threadIdx.x >> 5]);
+      sssp_task(qd, s_pre, nslots, total, local, __ldcg(&rd->sssp_w), g, lane, ws, rd, s_hdr[threadIdx.x >> 5], wb);
     } else if (t == T_DP || t == T_HOP) {
       const uint32_t* S = t == T_DP ? s_dp : s_hop;
       const uint32_t slot = find_slot_s(S, nslots, local);
       const QDev& q = qd[slot];
       const uint32_t st = q.qbuf[q.in_idx][local - S[slot]];
       if (t == T_DP)
-        dp_item(q, g, st, lane, rd, slot);
+        dp_item(q, g, st, lane, rd, slot, ws, wb);
       else
-        hop_item(q, g, st, lane, rd, slot);
+        hop_item(q, g, st, lane, rd, slot, ws, wb);
     } else if (t == T_TOUR) {
       tour_warp(qd[find_slot(P, nslots, local)], lane);
     } else if (t == T_EXTRACT) {
       if (lane == 0) extract_one(qd[find_slot(P, nslots, local)], g);
     } else {
-      uint32_t it = local * 32u + lane;
+      const uint32_t it = local * 32u + lane;
+      bool toN = false, toF = false;
+      uint32_t slot = 0, item = 0;
       if (it < total) {
-        uint32_t slot = find_slot(P, nslots, it);
+        slot = find_slot(P, nslots, it);
         const QDev& q = qd[slot];
-        uint32_t idx = it - __ldcg(P + slot);
-        if (t == T_SPLIT)
-          split_item(q, q.qbuf[q.far_idx][idx]);
-        else if (t == T_SSEED)
-          sseed_item(q, __ldg(q.members + idx));
-        else
+        const uint32_t idx = it - __ldcg(P + slot);
+        if (t == T_SPLIT) {
+          item = q.qbuf[q.far_idx][idx];
+          split_item(q, item, toN, toF);
+        } else if (t == T_SSEED) {
+          const uint32_t m = __ldg(q.members + idx);
+          item = m >> 3;
+          sseed_item(q, m, toN);
+        } else {
           dseed_item(q, __ldg(q.members + idx));
+        }
       }
+      push_multi(toN, item, 0u, qd[slot], slot, lane);
+      push_multi(toF, item, 1u, qd[slot], slot, lane);
     }
   }
-  if (lane == 0) sssp_acc_flush(acc);
+  wb_flush(wb, lane);
+  if (lane == 0) ws_flush(ws);
 }
 
 // Heavy round kernel: the arc chunks k_light handed over this round (hub
@@ -1411,6 +1444,14 @@ __global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, cons
   const uint32_t ntasks = __ldcg(&rd->heavy_tasks) + nbig;
   __shared__ uint32_t s_lb[MAX_SLOTS + 1];
   __shared__ RelaxHdr s_hub[8];
+  __shared__ WarpStat s_ws[8];
+  __shared__ WarpBuf s_wb[8];
+  WarpStat& ws = s_ws[threadIdx.x >> 5];
+  WarpBuf& wb = s_wb[threadIdx.x >> 5];
+  if (lane == 0) {
+    ws_init(ws);
+    wb_init(wb);
+  }
   for (int i = threadIdx.x; i <= nslots; i += blockDim.x) s_lb[i] = __ldcg(pre + T_LB * (MAX_SLOTS + 1) + i);
   __syncthreads();
   const uint32_t n_lb = __ldcg(&rd->items[T_LB]);
@@ -1418,9 +1459,9 @@ __global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, cons
     if (task < nbig) {
       const uint4 it = __ldcg(rd->big + task);
       if (it.x & CH_GROW)
-        grow_chunk(qd, it, g, lane);
+        grow_chunk(qd, it, g, lane, ws, wb);
       else
-        hub_chunk(qd, it, g, lane, &s_hub[threadIdx.x >> 5]);
+        hub_chunk(qd, it, g, lane, &s_hub[threadIdx.x >> 5], ws, wb);
       continue;
     }
     const uint32_t it = (task - nbig) * 4u + (lane >> 3);
@@ -1430,6 +1471,8 @@ __global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, cons
       lbt_row8(ql, ql.lb_off + (it - s_lb[slot]), lane & 7u);
     }
   }
+  wb_flush(wb, lane);
+  if (lane == 0) ws_flush(ws);
 }
 
 }  // namespace gstb

@@ -37,7 +37,10 @@ KMAX = 8
 class GstError(RuntimeError):
     def __init__(self, status: int, what: str = ""):
         self.status = status
-        super().__init__(f"{what}: {STATUS_NAMES.get(status, status)}")
+        detail = ""
+        if status == GST_CUDA_ERROR and _lib is not None:
+            detail = f" ({_lib.gst_last_cuda_error().decode()})"
+        super().__init__(f"{what}: {STATUS_NAMES.get(status, status)}{detail}")
 
 
 class _Result(ctypes.Structure):
@@ -67,6 +70,8 @@ def lib():
         L.gst_query_noalloc.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Result)]
         L.gst_query_noalloc.restype = ctypes.c_int
         L.gst_status_string.restype = ctypes.c_char_p
+        L.gst_last_cuda_error.restype = ctypes.c_char_p
+        L.gst_last_cuda_error.argtypes = []
         L.gst_graph_num_vertices.restype = u32
         L.gst_graph_num_vertices.argtypes = [vp]
         L.gst_graph_num_arcs.restype = u64

@@ -172,6 +172,9 @@ gst_status gst_serve_poll(gst_server* s, uint64_t* ids, int32_t* statuses, gst_r
 gst_status gst_serve_close(gst_server* s);
 
 const char* gst_status_string(gst_status st);
+/* The CUDA runtime's description of the last CUDA error any gstb call in this
+ * process met (the detail behind GST_CUDA_ERROR); "no error" if none. */
+const char* gst_last_cuda_error(void);
 
 /* Diagnostics (no reference counterpart).  Kernel launches issued by this
  * graph's engine so far, and, when profiling is on (gst_query_batch calls
