@@ -7,11 +7,15 @@
 //                              INF = all ones (memset 0xFF); a 64-bit atomicMin keeps
 //                              cost and parent consistent (no torn parents, unlike the
 //                              reference's separate stores at DPQ.cu:117-121).
-//   dist   u32 [V][8]          shortest distance from query group j to v
+//   dist   u32 [V][8]          one 32-byte sector per vertex: words 0..6 the
+//                               shortest distance from query group j to v,
+//                               word 7 the groups of v pending in the near list
+//                               (bits 0-7 and 8-15: the two round parities) and
+//                               in the far list (bits 16-23).  A relaxation
+//                               reads the target's distances and flags with one
+//                               sector load and updates both in that sector.
 //   dflag  u32 [ceil(V*2^k*nd/8)]   4 bits per state: in-near (two round
 //                                   parities), in-far
-//   sflag  u32 [3][V]              per vertex: groups pending in the near list
-//                                   (two round parities) and in the far list
 //   qbuf   u32 [4][cap]        near-in, near-out, far, far-out work lists of state ids
 //   tour   u32 [k][2^k][k] + [k][2^k] + [8][8]  tour tables P, T2 and group distances
 //   lbt    u16 [V][2^k]        lower bound of completing (v, X) to every group
@@ -25,7 +29,11 @@ constexpr unsigned long long INF64 = 0xFFFFFFFFFFFFFFFFull;
 constexpr uint32_t BIG = 1u << 30;  // saturation value inside lower-bound sums
 constexpr uint32_t PAR_GROW = 0x40000000u;
 constexpr uint32_t PAR_MERGE = 0x80000000u;
-constexpr int KMAX = 8;
+constexpr int KMAX = 7;        // query groups at most (word 7 of a distance row holds flags)
+constexpr int ROW = 8;         // words per distance row
+constexpr int FLAGW = 7;       // the pending-flags word of a row
+constexpr uint32_t FAR_SH = 16;  // far-list byte of the flags word
+__device__ __forceinline__ uint32_t near_sh(uint32_t par) { return par * 8u; }  // near-list byte of a parity
 constexpr int DMAX = 7;
 
 // Job state machine (advanced on the device by k_control once per round).
@@ -114,7 +122,6 @@ struct QDev {
   unsigned long long* table;
   uint32_t* dist;
   uint32_t* dflag;
-  uint32_t* sflag;
   uint32_t* qbuf[4];
   uint32_t* tour;
   unsigned short* lbt;      // [V][2^k] lower bound per (vertex, uncovered set)

@@ -236,7 +236,7 @@ class Arena {
 
 // Workspace layout of one query (see gst_device.cuh).
 struct Layout {
-  size_t table, dist, dflag, sflag, qbuf, tour, lbt, members, edges, total;
+  size_t table, dist, dflag, qbuf, tour, lbt, members, edges, total;
   uint32_t cap;
 };
 
@@ -258,7 +258,6 @@ Layout layout_for(const gst_graph* g, int k, int nd, size_t n_members, uint32_t 
   L.table = o; o = align_up(o + states * 8, 256);
   L.dist = o; o = align_up(o + (size_t)g->V * 8 * 4, 256);
   L.dflag = o; o = align_up(o + ((states + 7) / 8) * 4, 256);
-  L.sflag = o; o = align_up(o + (size_t)g->V * 3 * 4, 256);
   L.qbuf = o; o = align_up(o + 4 * cap * 4, 256);
   L.tour = o; o = align_up(o + ((size_t)k * (1u << k) * k + (size_t)k * (1u << k) + 64) * 4, 256);
   L.lbt = o; o = align_up(o + (size_t)g->V * (1u << k) * 2, 256);
@@ -431,7 +430,6 @@ class Runner {
     q.table = (unsigned long long*)(j->mem + L.table);
     q.dist = (uint32_t*)(j->mem + L.dist);
     q.dflag = (uint32_t*)(j->mem + L.dflag);
-    q.sflag = (uint32_t*)(j->mem + L.sflag);
     for (int b = 0; b < 4; b++) q.qbuf[b] = (uint32_t*)(j->mem + L.qbuf) + (size_t)b * L.cap;
     q.tour = (uint32_t*)(j->mem + L.tour);
     q.lbt = (unsigned short*)(j->mem + L.lbt);
@@ -462,9 +460,10 @@ class Runner {
     j->ctl.best = INF32;
     j->ctl.best_full = INF64;
     cudaMemsetAsync(q.table, 0xFF, (size_t)g_->V * j->WT * 8, stream_);
-    cudaMemsetAsync(q.dist, 0xFF, (size_t)g_->V * 8 * 4, stream_);
-    cudaMemsetAsync(q.dflag, 0, L.sflag - L.dflag, stream_);
-    cudaMemsetAsync(q.sflag, 0, L.qbuf - L.sflag, stream_);
+    // distances unknown, no group pending (word FLAGW of every row)
+    cudaMemsetAsync(q.dist, 0xFF, (size_t)g_->V * ROW * 4, stream_);
+    cudaMemset2DAsync(q.dist + FLAGW, ROW * 4, 0, 4, g_->V, stream_);
+    cudaMemsetAsync(q.dflag, 0, L.qbuf - L.dflag, stream_);
     // stage the member list and both descriptors in pinned memory; it is not
     // reused before the stream synchronises at the end of the next round block
     char* st = h_stage_ + (size_t)sh * (stage_cap_ / 2) + stage_off_[sh];
@@ -930,7 +929,7 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
       j.rejected = true;
       continue;
     }
-    memcpy(j.groups, groups + (size_t)i * KMAX, (size_t)j.k * 4);
+    memcpy(j.groups, groups + (size_t)i * GST_GROUPS_STRIDE, (size_t)j.k * 4);
     j.t_submit = std::chrono::steady_clock::now();
     gst_status ps = R.prepare(&j);
     if (ps != GST_OK) {
@@ -1243,7 +1242,6 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   q.table = (unsigned long long*)(ws + L.table);
   q.dist = (uint32_t*)(ws + L.dist);
   q.dflag = (uint32_t*)(ws + L.dflag);
-  q.sflag = (uint32_t*)(ws + L.sflag);
   for (int b = 0; b < 4; b++) q.qbuf[b] = (uint32_t*)(ws + L.qbuf) + (size_t)b * L.cap;
   q.tour = (uint32_t*)(ws + L.tour);
   q.lbt = (unsigned short*)(ws + L.lbt);
@@ -1278,9 +1276,9 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   auto t0 = std::chrono::steady_clock::now();
   // the array keeps the previous call's contents: reset what must start empty
   CK(cudaMemsetAsync(q.table, 0xFF, (size_t)g->V * WT * 8, 0));
-  CK(cudaMemsetAsync(q.dist, 0xFF, (size_t)g->V * 8 * 4, 0));
-  CK(cudaMemsetAsync(q.dflag, 0, L.sflag - L.dflag, 0));
-  CK(cudaMemsetAsync(q.sflag, 0, L.qbuf - L.sflag, 0));
+  CK(cudaMemsetAsync(q.dist, 0xFF, (size_t)g->V * ROW * 4, 0));
+  CK(cudaMemset2DAsync(q.dist + FLAGW, ROW * 4, 0, 4, g->V, 0));
+  CK(cudaMemsetAsync(q.dflag, 0, L.qbuf - L.dflag, 0));
   // grids: every SM filled to the occupancy limit of each kernel
   int bl = 0, bh = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, k_light, 256, 0));

@@ -603,10 +603,8 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
   const uint32_t lo_end = __shfl_sync(FULL, x, i0 == 0u ? 0u : i0 - 1u);
   const uint32_t f0 = i0 == 0u ? 0u : lo_end;
   const uint32_t f1 = __shfl_sync(FULL, x, i1 - 1u);
-  const uint32_t V = q.nv, thi = q.theta_hi;
+  const uint32_t thi = q.theta_hi, nsh = near_sh(q.par ^ 1u);
   uint32_t* __restrict__ dist = q.dist;
-  uint32_t* pnext = q.sflag + (size_t)(q.par ^ 1u) * V;
-  uint32_t* pfar = q.sflag + (size_t)2 * V;
   for (uint32_t base = f0; base < f1; base += 32u * SSSP_U) {
     uint2 arc[SSSP_U];
     uint32_t itm[SSSP_U];
@@ -649,14 +647,14 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
         cnt.arcs++;
         const RelaxHdr& hh = h[itm[u]];
         const uint32_t rm = hh.rm;
-        const uint32_t du[8] = {ra[u].x, ra[u].y, ra[u].z, ra[u].w, rb[u].x, rb[u].y, rb[u].z, rb[u].w};
+        const uint32_t du[KMAX] = {ra[u].x, ra[u].y, ra[u].z, ra[u].w, rb[u].x, rb[u].y, rb[u].z};
 #pragma unroll
         for (int t = 0; t < KMAX; t++) {
           if ((rm >> t) & 1u) {
             const uint32_t dt = hh.d[t];
             const uint32_t nd = dt + arc[u].y;
             if (nd >= dt && nd <= capb && nd < du[t]) {
-              atomicMin(dist + (size_t)arc[u].x * 8 + t, nd);  // result not needed
+              atomicMin(dist + (size_t)arc[u].x * ROW + t, nd);  // result not needed
               if (nd < thi)
                 nn[u] |= 1u << t;
               else
@@ -667,19 +665,23 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
         }
       }
     }
-    // all flag updates of the step are issued before any result is used
-    uint32_t oN[SSSP_U], oF[SSSP_U], itv[SSSP_U];
+    // flags: one atomicOr per target for both lists, skipped when the row
+    // just read shows the bits set already (a hub's flags are then not hit
+    // by every relaxation that lowers it); all of the step's flag updates are
+    // issued before any result is used
+    uint32_t old[SSSP_U], itv[SSSP_U];
 #pragma unroll
     for (int u = 0; u < SSSP_U; u++) {
-      oN[u] = nn[u] ? atomicOr(pnext + arc[u].x, nn[u]) : 1u;
-      oF[u] = nf[u] ? atomicOr(pfar + arc[u].x, nf[u]) : 1u;
+      const uint32_t bits = (nn[u] << nsh) | (nf[u] << FAR_SH);
+      const uint32_t fw = rb[u].w;
+      old[u] = (bits & ~fw) ? atomicOr(dist + (size_t)arc[u].x * ROW + FLAGW, bits) : fw;
       itv[u] = arc[u].x;
     }
     bool tN[SSSP_U], tF[SSSP_U];
 #pragma unroll
     for (int u = 0; u < SSSP_U; u++) {
-      tN[u] = oN[u] == 0u;
-      tF[u] = oF[u] == 0u;
+      tN[u] = nn[u] && ((old[u] >> nsh) & 0xFFu) == 0u;
+      tF[u] = nf[u] && ((old[u] >> FAR_SH) & 0xFFu) == 0u;
     }
     cnt.enq += append_lists<SSSP_U>(tN, tF, itv, q, lane, wb);
   }
@@ -707,12 +709,14 @@ __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restric
   bool active = false;
   if (valid) {
     const QDev& q = qd[slot];
-    const uint32_t V = q.nv;
     const int k = q.k;
     const uint32_t v = q.qbuf[q.in_idx][it - pre[slot]];
-    // the header's loads depend on v only, so they are all in flight at once
-    const uint32_t m = atomicExch(&q.sflag[(size_t)q.par * V + v], 0u);
-    const uint4* drow = reinterpret_cast<const uint4*>(q.dist + (size_t)v * 8);
+    // the header's loads depend on v only, so they are all in flight at once;
+    // take the groups pending at v for this round's parity
+    const uint32_t psh = near_sh(q.par);
+    const uint32_t m =
+        (atomicAnd(q.dist + (size_t)v * ROW + FLAGW, ~(0xFFu << psh)) >> psh) & 0xFFu;
+    const uint4* drow = reinterpret_cast<const uint4*>(q.dist + (size_t)v * ROW);
     const uint4 da = __ldcg(drow), db = __ldcg(drow + 1);
     uint32_t best = ld_best(q.ctl);
     const uint32_t b0 = __ldg(g.beg + v), b1 = __ldg(g.beg + v + 1);
@@ -722,7 +726,7 @@ __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restric
       wa = __ldg(wr);
       wb = __ldg(wr + 1);
     }
-    const uint32_t d[8] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z, db.w};
+    const uint32_t d[KMAX] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z};
     // star bound at v (unbounded queries only): v joined to every group by
     // shortest paths is a feasible tree (one-label completion, CPUNONHOP.h:684-699)
     if (q.D < 0) {
@@ -823,10 +827,10 @@ __device__ void hub_chunk(const QDev* __restrict__ qd, const uint4 item, const G
   const QDev& q = qd[slot];
   uint32_t capb = 0, n = 0;
   if (lane == 0) {
-    const uint4* drow = reinterpret_cast<const uint4*>(q.dist + (size_t)v * 8);
+    const uint4* drow = reinterpret_cast<const uint4*>(q.dist + (size_t)v * ROW);
     const uint4 da = __ldcg(drow), db = __ldcg(drow + 1);
     const uint32_t best = ld_best(q.ctl);
-    const uint32_t d[8] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z, db.w};
+    const uint32_t d[KMAX] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z};
     capb = (uint32_t)((unsigned long long)best * q.cap_num / q.cap_den);
     uint32_t rm = 0, dmin = INF32;
 #pragma unroll
@@ -901,21 +905,27 @@ __device__ void split_item(const QDev& q, uint32_t s, bool& toN, bool& toF) {
   uint32_t best = ld_cg(&q.ctl->best);
   toN = toF = false;
   if (q.phase == PH_SSSP) {
-    const uint32_t V = q.nv;
+    uint32_t* fw = q.dist + (size_t)s * ROW + FLAGW;
     const uint32_t capb = (uint32_t)((unsigned long long)best * q.cap_num / q.cap_den);
-    uint32_t fm = atomicExch(&q.sflag[(size_t)2 * V + s], 0u);
+    const uint32_t fm = (atomicAnd(fw, ~(0xFFu << FAR_SH)) >> FAR_SH) & 0xFFu;
     uint32_t nb = 0, kb = 0;
     for (int t = 0; t < q.k; t++) {
       if (!((fm >> t) & 1u)) continue;
-      uint32_t d = ld_cg(q.dist + (size_t)s * 8 + t);
+      uint32_t d = ld_cg(q.dist + (size_t)s * ROW + t);
       if (d < q.theta_lo || d == INF32 || d > capb) continue;
       if (d < q.theta_hi)
         nb |= 1u << t;
       else
         kb |= 1u << t;
     }
-    toN = nb && atomicOr(&q.sflag[(size_t)q.par * V + s], nb) == 0u;
-    toF = kb && atomicOr(&q.sflag[(size_t)2 * V + s], kb) == 0u;
+    // items moved to the near list carry the next round's parity, which a
+    // split round does not flip
+    const uint32_t psh = near_sh(q.par);
+    if (nb | kb) {
+      const uint32_t old = atomicOr(fw, (nb << psh) | (kb << FAR_SH));
+      toN = nb && ((old >> psh) & 0xFFu) == 0u;
+      toF = kb && ((old >> FAR_SH) & 0xFFu) == 0u;
+    }
     return;
   }
   uint32_t cost = (uint32_t)(ld_cg(q.table + s) >> 32);
@@ -935,8 +945,9 @@ __device__ void split_item(const QDev& q, uint32_t s, bool& toN, bool& toF) {
 // (the caller pushes v if toN).
 __device__ void sseed_item(const QDev& q, uint32_t item, bool& toN) {
   uint32_t v = item >> 3, j = item & 7u;
-  q.dist[item] = 0;
-  toN = atomicOr(&q.sflag[(size_t)q.par * q.nv + v], 1u << j) == 0u;
+  q.dist[(size_t)v * ROW + j] = 0;
+  const uint32_t psh = near_sh(q.par);
+  toN = ((atomicOr(q.dist + (size_t)v * ROW + FLAGW, (1u << j) << psh) >> psh) & 0xFFu) == 0u;
 }
 
 // Single append (DP seeding only: once per member state of a query).

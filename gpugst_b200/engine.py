@@ -31,7 +31,8 @@ STATUS_NAMES = {0: "ok", 1: "no solution", 2: "bad input", 3: "out of memory", 4
 STAT_NAMES = ["expanded", "sssp_items", "arcs", "updates", "enqueued", "rounds", "merges", "table_bytes",
               "sssp_arcs", "sssp_updates", "sssp_enqueued", "retries"]
 NSTATS = len(STAT_NAMES)
-KMAX = 8
+GROUPS_STRIDE = 8  # row stride of gst_query_batch's groups array
+KMAX = 7           # query groups at most
 
 
 class GstError(RuntimeError):
@@ -208,7 +209,7 @@ class Engine:
     def query_batch(self, queries, Ds=None, max_concurrent: int = 0, max_edges: int = 4096):
         """Many queries sharing device rounds (gst_query_batch)."""
         n = len(queries)
-        groups = np.zeros((n, KMAX), dtype=np.uint32)
+        groups = np.zeros((n, GROUPS_STRIDE), dtype=np.uint32)
         ks = np.zeros(n, dtype=np.int32)
         for i, q in enumerate(queries):
             ks[i] = len(q)

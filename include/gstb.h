@@ -20,7 +20,7 @@
  *
  * Conventions: plain pointers and sizes only; the caller owns every host
  * buffer; the library owns every device buffer.  Costs are int32 edge-weight
- * sums; vertex ids are uint32; a query names k (1..8) group indices (0-based,
+ * sums; vertex ids are uint32; a query names k (1..7) group indices (0-based,
  * i.e. the `.g` file id minus one, as read_Group does at
  * graph_hash_of_mixed_weighted_read_for_GSTP.h:206).  D < 0 means no hop bound;
  * 0 <= D <= 7 bounds the tree's hop diameter (the recurrence of
@@ -138,6 +138,9 @@ gst_status gst_query(gst_graph* g, const uint32_t* groups, int k, int D, gst_res
  * caller's current device before returning. */
 #define GST_NOALLOC_SCRATCH_BYTES (64ull << 20)
 gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, int k, int D, gst_result* out);
+
+/* Row stride of the groups array of gst_query_batch. */
+#define GST_GROUPS_STRIDE 8
 
 /* Batched launch: n queries share the device rounds.  groups[i*8 .. i*8+ks[i])
  * lists query i's groups.  results[i].edges/max_edges set by the caller.

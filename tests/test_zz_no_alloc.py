@@ -42,7 +42,7 @@ def test_noalloc_rejects_oversized_query(gst_lib):
     eng = gst_lib
     g, gr, qs = gen.config1()
     E = eng.Engine.from_instance(g, gr)
-    q = np.arange(8, dtype=np.uint32)  # 10,000 x 2^8 x 8 states: a 164 MB state table
+    q = np.arange(7, dtype=np.uint32)  # 10,000 x 2^7 x 8 states: an 82 MB state table
     r = E.query_noalloc(q, D=7)
     assert r.status == eng.GST_SCRATCH_TOO_SMALL
     # a fitting query still works afterwards
