@@ -147,6 +147,8 @@ struct QDev {
   uint32_t delta, delta_sssp, delta_dp;
   uint32_t par;      // parity of the items in (or entering) the near list
   uint32_t lb_off;   // bound-table rows (vertices) already computed
+  uint32_t hops;     // distance rounds done (hop-bounded queries stop after D)
+  uint32_t pad_h;
 };
 
 struct GraphDev {

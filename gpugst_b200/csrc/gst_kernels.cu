@@ -36,6 +36,14 @@ __device__ __forceinline__ uint32_t warp_sum(uint32_t x) {
   return x;
 }
 
+// Bound-table entries: LB_INF marks a completion that is impossible (a group
+// out of reach); finite bounds saturate at LB_INF - 1, which stays a valid
+// lower bound.
+constexpr uint32_t LB_INF = 0xFFFFu;
+__device__ __forceinline__ bool lb_ok(uint32_t cost, uint32_t lb, uint32_t best) {
+  return lb != LB_INF && (unsigned long long)cost + lb <= best;
+}
+
 // Statistics of the query a warp is working for, kept in shared memory by
 // lane 0 and added to the query's counters only when the warp moves to
 // another query and at kernel end (one atomic per event would queue on the
@@ -255,7 +263,7 @@ __device__ __forceinline__ void grow_arcs(const QDev& q, const GraphDev& g, uint
 #pragma unroll
     for (int u = 0; u < GROW_U; u++) {
       nc[u] = c + arc[u].y;
-      want[u] = ok[u] && nc[u] < cur[u] && (unsigned long long)nc[u] + lbu[u] <= best;
+      want[u] = ok[u] && nc[u] < cur[u] && lb_ok(nc[u], lbu[u], best);
       if (ok[u]) cnt.arcs++;
       if (want[u]) {
         // the pre-check already saw a higher cost: enqueue on it and let the
@@ -377,7 +385,7 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
   best = __shfl_sync(FULL, best, 0);
   const unsigned short* lbt = q.lbt;
   uint32_t lbv = __ldg(lbt + ((size_t)v << k) + comp);
-  if ((unsigned long long)c + lbv > best) return;
+  if (!lb_ok(c, lbv, best)) return;
 
   GrowCnt gc;
   // grow, only from states of cost <= best/2 (optimal-tree decomposition,
@@ -412,7 +420,7 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
           // conditional tree merging: 3m <= 2 best (CPUNONHOP.h:941)
           if (3ull * m <= 2ull * best && m < cq) {
             uint32_t lbq = __ldg(lbt + ((size_t)v << k) + (full ^ qset));
-            if (m + lbq <= best) {
+            if (lb_ok((uint32_t)m, lbq, best)) {
               m32 = (uint32_t)m;
               t = (v << k) | qset;
               atomicMin(q.table + t, pack(m32, PAR_MERGE | p));
@@ -463,7 +471,7 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
   if (lane == 0) ws_add(ws, q.ctl, ST_EXPANDED, 1u);
   const unsigned short* lbt = q.lbt;
   uint32_t lbv = __ldg(lbt + ((size_t)v << k) + comp);
-  if ((unsigned long long)c + lbv > best) return;
+  if (!lb_ok(c, lbv, best)) return;
   GrowCnt gc;
   if (d < (uint32_t)D) {  // grow d -> d+1 (CPUHOP.h:192-206)
     const uint32_t lim = best - c;
@@ -507,7 +515,7 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
               if (m32 < best) atomicMin(&q.ctl->best, m32);
             } else {
               uint32_t lbq = __ldg(lbt + ((size_t)v << k) + (full ^ qset));
-              if (m + lbq <= best && m32 < (uint32_t)(ld_cg(q.table + t) >> 32)) {
+              if (lb_ok(m32, lbq, best) && m32 < (uint32_t)(ld_cg(q.table + t) >> 32)) {
                 atomicMin(q.table + t, pack(m32, par));
                 want = true;
                 gc.upd++;
@@ -882,7 +890,7 @@ __device__ void grow_chunk(const QDev* __restrict__ qd, const uint4 item, const 
   c = __shfl_sync(FULL, c, 0);
   best = __shfl_sync(FULL, best, 0);
   lbv = __shfl_sync(FULL, lbv, 0);
-  if (c == INF32 || c > best || (unsigned long long)c + lbv > best) return;
+  if (c == INF32 || c > best || !lb_ok(c, lbv, best)) return;
   if (!hop && 2ull * c > best) return;
   GrowCnt gc;
   grow_arcs(q, g, lane, v, p, comp, c, best, best - c, hop ? (int)d + 1 : -1, item.z, item.w, gc, wb);
@@ -1051,8 +1059,10 @@ __device__ void lbt_row8(const QDev& q, uint32_t v, uint32_t sl) {
 #pragma unroll
   for (int j = 0; j < KMAX; j++) dl[j] = min(r[j], q.cap1);
   unsigned short* out = q.lbt + ((size_t)v << k);
-  for (uint32_t X = sl; X < K2; X += 8)
-    out[X] = X == 0 ? (unsigned short)0 : (unsigned short)min(lower_bound_comp(dl, k, X, P, T2), 65535u);
+  for (uint32_t X = sl; X < K2; X += 8) {
+    const uint32_t lb = X == 0 ? 0u : lower_bound_comp(dl, k, X, P, T2);
+    out[X] = (unsigned short)(lb >= BIG ? LB_INF : min(lb, LB_INF - 1u));
+  }
 }
 
 // Weight of arc (a -> b): linear scan of a's weight-sorted adjacency.
@@ -1167,6 +1177,7 @@ __device__ __forceinline__ void absorb(QDev& q, QCtl& c) {
       q.n_in = c.n_near;
       q.n_far = c.n_far;
       q.par ^= 1u;  // producers of the round flagged the next items with the other parity
+      if (q.st == J_SSSP) q.hops++;
       break;
     case A_SPLIT:
       t = q.in_idx; q.in_idx = q.out_idx; q.out_idx = t;
@@ -1206,13 +1217,26 @@ __device__ __forceinline__ void decide(QDev& q, QCtl& c) {
       case J_INIT:
         q.phase = PH_SSSP;
         q.theta_lo = 0;
-        q.theta_hi = q.delta_sssp;
+        // a hop-bounded query runs its distance rounds as Bellman-Ford rounds
+        // (one window holding everything): after D rounds every path of at
+        // most D hops has been relaxed
+        q.theta_hi = q.D >= 0 ? INF32 : q.delta_sssp;
         q.delta = q.delta_sssp;
+        q.hops = 0;
         c.n_near = 0;
         q.act = A_SSEED;
         return;
       case J_SSSP:
       case J_DP: {
+        if (q.st == J_SSSP && q.D >= 0 && q.hops >= (uint32_t)q.D) {
+          // hop-bounded distances: d_j(v) <= the cheapest path of at most D
+          // hops from group j to v, INF if there is none.  Every path of the
+          // final tree has at most D hops, so these are valid lower bounds,
+          // and an unreached vertex cannot join a group
+          q.cap1 = BIG;
+          q.st = J_TOUR;
+          continue;
+        }
         if (q.n_in > 0) {
           c.n_near = 0;
           c.n_far = q.n_far;
