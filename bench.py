@@ -131,30 +131,33 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-# Algorithmic bytes of the two round kernels, from their device counters
-# (the useful bytes each unit of work must move):
-#   k_light, distance item  : 48 B per vertex (item id 4, pending mask 4,
-#                             distance row 32, adjacency offsets 8)
-#            per arc        : 40 B ({neighbour, weight} 8 + target distance row 32)
-#            per update / enqueue : 4 B / 8 B (mask 4 + list entry 4)
-#   k_heavy, DP state       : 66 B (item id 4, flag 4, state word 8, distance
-#                             row 32, complement word 8, bound 2, offsets 8)
-#            per arc        : 18 B ({neighbour, weight} 8, target word 8, bound 2)
+# Algorithmic bytes of a round, from the device counters (the useful bytes
+# each unit of work must move).  The two round kernels share the work types
+# (k_light: distance items and DP states; k_heavy: the arc chunks k_light
+# hands over and the bound-table rows), so the round is the unit measured.
+#   distance item       : 48 B per vertex (item id 4, flags 4, distance row
+#                         32, adjacency offsets 8)
+#            per arc    : 40 B ({neighbour, weight} 8 + target distance row 32,
+#                         whose word 7 holds the pending-group flags)
+#            per update / enqueue : 4 B / 8 B (flags 4 + list entry 4)
+#   DP state            : 66 B (item id 4, flag 4, state word 8, distance
+#                         row 32, complement word 8, bound 2, offsets 8)
+#            per arc    : 18 B ({neighbour, weight} 8, target word 8, bound 2)
 #            per merge partner : 10 B (word 8, bound 2); update 8 B; enqueue 8 B
-#            per bound row  : 32 B read + 2 * 2^k B written (one per vertex)
-def light_bytes(st):
+#   bound row           : 32 B read + 2 * 2^k B written (one per vertex)
+def distance_work_bytes(st):
     return 48 * st["sssp_items"] + 40 * st["sssp_arcs"] + 4 * st["sssp_updates"] + 8 * st["sssp_enqueued"]
 
 
-def heavy_bytes(st, V, ks):
+def dp_work_bytes(st, V, ks):
     lb_rows = sum(V * (32 + 2 * (1 << k)) for k in ks)
     return (66 * st["expanded"] + 18 * st["arcs"] + 10 * st["merges"] + 8 * st["updates"]
             + 8 * st["enqueued"] + lb_rows)
 
 
 def traffic_per_byte():
-    """DRAM bytes per algorithmic byte of the dominant round kernel, from the
-    committed ncu summary (profiles/round_kernel_traffic.json), if present."""
+    """DRAM bytes per algorithmic byte of a round (both round kernels), from
+    the committed ncu summary (profiles/round_kernel_traffic.json), if present."""
     p = os.path.join(ROOT, "profiles", "round_kernel_traffic.json")
     if not os.path.exists(p):
         return None
@@ -378,15 +381,14 @@ def main():
     E.query_batch(prof_batch)
     light_ms, heavy_ms, prof_rounds, st = E.profile_read()
     E.profile(False)
-    lb_bytes = light_bytes(st)
-    hb_bytes = heavy_bytes(st, g.V, [len(q) for q in prof_batch])
+    dist_bytes = distance_work_bytes(st)
+    dp_bytes = dp_work_bytes(st, g.V, [len(q) for q in prof_batch])
     peak, peak_kind = measured_peak_hbm()
-    kern = {"k_light": (light_ms, lb_bytes), "k_heavy": (heavy_ms, hb_bytes)}
-    dom = max(kern, key=lambda n: kern[n][0])
-    dom_ms, dom_bytes = kern[dom]
-    achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    round_ms = light_ms + heavy_ms
+    round_bytes = dist_bytes + dp_bytes
+    achieved = round_bytes / (round_ms / 1e3) / 1e9 if round_ms > 0 else 0.0
     tpb = traffic_per_byte()
-    per_launch_alg = dom_bytes / max(prof_rounds, 1)
+    per_round_alg = round_bytes / max(prof_rounds, 1)
 
     # continuous-batching serving loop (closed loop, `--inflight` requests on the device)
     n_serve = args.serve
@@ -457,12 +459,12 @@ def main():
             "serve_vs_plain": serve_qps / plain_qps if (plain_qps and serve_qps) else None,
             "serve": {"value": serve_qps, "unit": "queries/s", "inflight": args.inflight, "queries": n_serve,
                       "p50_ms": pct(lat_serve, 50), "p99_ms": pct(lat_serve, 99)},
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": (per_launch_alg * tpb) if tpb else None,
-                         "algorithmic_bytes_per_launch": per_launch_alg, "launches": prof_rounds,
+            "roofline": {"bound": "hbm", "kernel": "round (k_light + k_heavy)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": (per_round_alg * tpb) if tpb else None,
+                         "algorithmic_bytes_per_round": per_round_alg, "rounds": prof_rounds,
                          "kernel_ms": {"k_light": light_ms, "k_heavy": heavy_ms},
-                         "algorithmic_bytes": {"k_light": lb_bytes, "k_heavy": hb_bytes}},
+                         "algorithmic_bytes": {"distance": dist_bytes, "dp": dp_bytes}},
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": int(launches),

@@ -287,7 +287,7 @@ class Runner {
     for (auto& hh : ev_prof_)
       for (auto& e : hh) CK(cudaEventCreate(&e));
     delta_sssp_ = std::max(1u, env_u32("GSTB_DELTA_SSSP", 16));
-    delta_dp_ = std::max(1u, env_u32("GSTB_DELTA_DP", 4));
+    delta_dp_ = std::max(1u, env_u32("GSTB_DELTA_DP", 8));
     cap_num_ = std::max(1u, env_u32("GSTB_SSSP_CAP_NUM", 1));
     cap_den_ = std::max(1u, env_u32("GSTB_SSSP_CAP_DEN", 2));
     max_edges_dev_ = env_u32("GSTB_MAX_TREE_EDGES", 1u << 16);
@@ -1267,7 +1267,7 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   q.st = J_INIT;
   q.act = A_NONE;
   q.delta_sssp = std::max(1u, env_u32("GSTB_DELTA_SSSP", 16));
-  q.delta_dp = std::max(1u, env_u32("GSTB_DELTA_DP", 4));
+  q.delta_dp = std::max(1u, env_u32("GSTB_DELTA_DP", 8));
   QCtl c;
   memset(&c, 0, sizeof(c));
   c.best = INF32;
