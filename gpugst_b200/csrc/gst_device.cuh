@@ -174,6 +174,17 @@ __device__ __forceinline__ unsigned long long pack(uint32_t cost, uint32_t par) 
   return ((unsigned long long)cost << 32) | par;
 }
 
+// Fire-and-forget reductions (PTX red): the issuing warp never waits for them.
+__device__ __forceinline__ void red_min(uint32_t* p, uint32_t v) {
+  asm volatile("red.relaxed.gpu.global.min.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void red_min(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.min.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void red_or(uint32_t* p, uint32_t v) {
+  asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ uint32_t ld_cg(const uint32_t* p) { return __ldcg(p); }
 // The incumbent through L1: a value cached earlier in the same launch can be
 // higher than the current one, which only weakens pruning (every use of best

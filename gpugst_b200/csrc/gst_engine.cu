@@ -175,6 +175,8 @@ class Arena {
     return grow(align_up(n - free_total_, 256), true);
   }
 
+  size_t free_bytes() const { return free_total_; }
+
   void release() {
     for (auto& c : chunks_) cudaFree(c.first);
     chunks_.clear();
@@ -405,6 +407,7 @@ class Runner {
 
   bool has_free_slot() const { return n_used_ < max_slots_; }
   bool reserve(size_t bytes) { return arena_.reserve(bytes); }
+  bool has_free(size_t bytes) const { return arena_.free_bytes() >= bytes; }
   size_t live() const { return n_used_; }
 
   // Allocate the workspace, initialise it and install the job in a free
@@ -490,6 +493,7 @@ class Runner {
   }
 
   double last_call_ms() const { return last_call_ms_; }
+  double trace_ms() const { return trace_ms_; }
 
   // Run rounds until no admitted job is left and admit_more() adds none.
   // `on_done` is called for every finished job (after its results are copied).
@@ -508,6 +512,8 @@ class Runner {
     int fin_half = 0;
     using clk = std::chrono::steady_clock;
     auto ms_since = [](clk::time_point a) { return std::chrono::duration<double, std::milli>(clk::now() - a).count(); };
+    double sum_admit = 0, sum_launch = 0, sum_fin = 0, sum_blk = 0, sum_all = 0;
+    int iters = 0;
     for (;;) {
       const clk::time_point t_it = clk::now();
       double t_admit = 0, t_launch = 0, t_fin = 0, t_blk = 0;
@@ -552,6 +558,12 @@ class Runner {
       }
       if (trace_ms_ > 0) {
         const double t_all = ms_since(t_it);
+        sum_admit += t_admit;
+        sum_launch += t_launch - t_admit;
+        sum_fin += t_fin - t_launch;
+        sum_blk += t_blk > 0 ? t_blk - t_fin : 0.0;
+        sum_all += t_all;
+        iters++;
         if (t_all >= trace_ms_)
           fprintf(stderr,
                   "gstb: slow host iteration %.2f ms (admit %.2f, launch %.2f, finalize %.2f, block wait %.2f; "
@@ -566,6 +578,12 @@ class Runner {
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
     last_call_ms_ = ms;
+    if (trace_ms_ > 0 && sum_all >= trace_ms_)
+      fprintf(stderr,
+              "gstb: run of %d host iterations: %.2f ms (admit %.2f, launch %.2f, finalize %.2f, block wait %.2f, "
+              "rest %.2f)\n",
+              iters, sum_all, sum_admit, sum_launch, sum_fin, sum_blk,
+              sum_all - sum_admit - sum_launch - sum_fin - sum_blk);
     return GST_OK;
   }
 
@@ -915,6 +933,8 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
     g->runner = nr;
   }
   Runner& R = *static_cast<Runner*>(g->runner);
+  using clk = std::chrono::steady_clock;
+  const clk::time_point t0 = clk::now();
   std::vector<Job> jobs(n);
   std::deque<Job*> pending;
   for (int i = 0; i < n; i++) {
@@ -952,10 +972,16 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
       if (cnt++ >= std::min<size_t>(maxc, MAX_SLOTS - 1)) break;
       need += align_up(j->bytes, 256);
     }
-    size_t fr = 0, tot = 0;
-    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) need = std::min(need, (size_t)(fr * 0.8));
-    R.reserve(need);  // best effort: admission still grows the arena or waits
+    // best effort: admission still grows the arena or waits.  The device is
+    // asked for its free memory only when the arena must grow (the query can
+    // take milliseconds)
+    if (!R.has_free(need)) {
+      size_t fr = 0, tot = 0;
+      if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) need = std::min(need, (size_t)(fr * 0.8));
+      R.reserve(need);
+    }
   }
+  const clk::time_point t1 = clk::now();
   gst_status rs = R.run(
       [&]() {
         while (!pending.empty() && R.live() < maxc && R.has_free_slot()) {
@@ -974,6 +1000,7 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
       },
       [&](Job*) {});
   if (rs != GST_OK) return rs;
+  const clk::time_point t2 = clk::now();
   for (int i = 0; i < n; i++) {
     Job& j = jobs[i];
     if (j.rejected) continue;
@@ -981,6 +1008,14 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
     if (j.res) j.res->device_ms = R.last_call_ms();
     if (g->profile)
       for (int t = 0; t < GST_NSTATS; t++) g->prof_stats[t] += j.ctl.stat[t];
+  }
+  const double tr = R.trace_ms();
+  if (tr > 0) {
+    auto ms = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+    const double all = ms(t0, clk::now());
+    if (all >= tr)
+      fprintf(stderr, "gstb: batch of %d: %.2f ms (prepare %.2f, run %.2f with %.2f on the device, results %.2f)\n", n,
+              all, ms(t0, t1), ms(t1, t2), R.last_call_ms(), ms(t2, clk::now()));
   }
   return GST_OK;
 }

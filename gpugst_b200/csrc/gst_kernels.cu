@@ -269,7 +269,7 @@ __device__ __forceinline__ void grow_arcs(const QDev& q, const GraphDev& g, uint
         // the pre-check already saw a higher cost: enqueue on it and let the
         // 64-bit min land without waiting for its result (a concurrent lower
         // write also enqueues; the flag keeps the list free of duplicates)
-        atomicMin(q.table + t[u], pack(nc[u], PAR_GROW | v));
+        red_min(q.table + t[u], pack(nc[u], PAR_GROW | v));
         cnt.upd++;
       }
     }
@@ -423,7 +423,7 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
             if (lb_ok((uint32_t)m, lbq, best)) {
               m32 = (uint32_t)m;
               t = (v << k) | qset;
-              atomicMin(q.table + t, pack(m32, PAR_MERGE | p));
+              red_min(q.table + t, pack(m32, PAR_MERGE | p));
               want = true;
               gc.upd++;
             }
@@ -516,7 +516,7 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
             } else {
               uint32_t lbq = __ldg(lbt + ((size_t)v << k) + (full ^ qset));
               if (lb_ok(m32, lbq, best) && m32 < (uint32_t)(ld_cg(q.table + t) >> 32)) {
-                atomicMin(q.table + t, pack(m32, par));
+                red_min(q.table + t, pack(m32, par));
                 want = true;
                 gc.upd++;
               }
@@ -662,7 +662,7 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
             const uint32_t dt = hh.d[t];
             const uint32_t nd = dt + arc[u].y;
             if (nd >= dt && nd <= capb && nd < du[t]) {
-              atomicMin(dist + (size_t)arc[u].x * ROW + t, nd);  // result not needed
+              red_min(dist + (size_t)arc[u].x * ROW + t, nd);
               if (nd < thi)
                 nn[u] |= 1u << t;
               else
@@ -673,23 +673,24 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
         }
       }
     }
-    // flags: one atomicOr per target for both lists, skipped when the row
-    // just read shows the bits set already (a hub's flags are then not hit
-    // by every relaxation that lowers it); all of the step's flag updates are
-    // issued before any result is used
-    uint32_t old[SSSP_U], itv[SSSP_U];
+    // flags: one fire-and-forget OR per target for both lists, skipped when
+    // the row just read shows the bits set already.  The list entry is taken
+    // when that row showed the list's byte empty.  Within a round the
+    // next-parity and far bytes only gain bits, so the first OR to reach a
+    // byte comes from a lane that read it empty: every newly pending vertex
+    // is appended at least once.  Two lanes that both read it empty append
+    // it twice; the consumer's atomicAnd hands the groups to one of them
+    // and the other finds none.  No lane waits for an atomic's result.
+    uint32_t itv[SSSP_U];
+    bool tN[SSSP_U], tF[SSSP_U];
 #pragma unroll
     for (int u = 0; u < SSSP_U; u++) {
       const uint32_t bits = (nn[u] << nsh) | (nf[u] << FAR_SH);
       const uint32_t fw = rb[u].w;
-      old[u] = (bits & ~fw) ? atomicOr(dist + (size_t)arc[u].x * ROW + FLAGW, bits) : fw;
+      if (bits & ~fw) red_or(dist + (size_t)arc[u].x * ROW + FLAGW, bits);
+      tN[u] = nn[u] && ((fw >> nsh) & 0xFFu) == 0u;
+      tF[u] = nf[u] && ((fw >> FAR_SH) & 0xFFu) == 0u;
       itv[u] = arc[u].x;
-    }
-    bool tN[SSSP_U], tF[SSSP_U];
-#pragma unroll
-    for (int u = 0; u < SSSP_U; u++) {
-      tN[u] = nn[u] && ((old[u] >> nsh) & 0xFFu) == 0u;
-      tF[u] = nf[u] && ((old[u] >> FAR_SH) & 0xFFu) == 0u;
     }
     cnt.enq += append_lists<SSSP_U>(tN, tF, itv, q, lane, wb);
   }
