@@ -64,7 +64,7 @@ struct RoundDesc {
   uint32_t hub_on;        // set by k_control for the current round
   uint32_t sssp_w;        // distance items per warp task this round (set by k_control)
   uint32_t light_warps;   // warps of one k_light launch (set by the host)
-  uint32_t pad3;
+  uint32_t nslots;        // 1 + the highest slot in use this round (set by k_control)
 };
 constexpr uint32_t HUB_CHUNK = 256;     // arcs per chunk (one warp)
 constexpr uint32_t LB_CHUNK = 1u << 22; // bound-table rows (vertices) per query per round

@@ -337,6 +337,10 @@ class Runner {
     CK(cudaMallocHost(&h_edge_stage_, edge_stage_cap_));
     memset(h_qd_, 0, sizeof(QDev));  // the zero descriptor that frees a slot
     slots_.assign(max_slots_, nullptr);
+    if (env_u32("GSTB_ROUND_GRAPH", 1)) {
+      gst_status gs = build_round_graph();
+      if (gs != GST_OK) return gs;
+    }
     return GST_OK;
   }
 
@@ -366,6 +370,8 @@ class Runner {
       for (auto& e : hh)
         if (e) cudaEventDestroy(e);
     if (stream_) cudaStreamSynchronize(stream_);
+    if (round_graph_) cudaGraphExecDestroy(round_graph_);
+    round_graph_ = nullptr;
     arena_.release();
     if (stream_) cudaStreamDestroy(stream_);
     d_qd_ = nullptr;
@@ -588,21 +594,48 @@ class Runner {
   }
 
  private:
-  gst_status launch_block(uint32_t R) {
+  // A block of rounds_per_sync_ rounds as one CUDA graph.  Its arguments are
+  // static: k_control scans every slot and publishes the bound the round
+  // kernels search, so the graph serves any set of admitted queries.
+  gst_status build_round_graph() {
     GraphDev gd{g_->d_beg, g_->d_adj, g_->V, g_->d_wcut};
-    const int ns = (int)nslots_hi_;
-    const unsigned light_grid = light_grid_, heavy_grid = heavy_grid_;
+    cudaGraph_t gr = nullptr;
+    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    for (uint32_t r = 0; r < rounds_per_sync_; r++) {
+      k_control<<<1, 1024, 0, stream_>>>(d_qd_, d_ctl_, (int)max_slots_, d_rd_, d_pre_);
+      k_light<<<light_grid_, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, MAX_SLOTS, gd);
+      k_heavy<<<heavy_grid_, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, MAX_SLOTS, gd);
+    }
+    const cudaError_t le = cudaGetLastError();
+    const cudaError_t ce = cudaStreamEndCapture(stream_, &gr);  // always leave capture mode
+    CK(le);
+    CK(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&round_graph_, gr, 0);
+    cudaGraphDestroy(gr);
+    CK(ie);
+    return GST_OK;
+  }
+
+  gst_status launch_block(uint32_t R) {
     const int h = (int)(next_block_ & 1);
     const bool prof = g_->profile;
-    cudaEvent_t* pe = ev_prof_[h];
-    for (uint32_t r = 0; r < R; r++) {
-      k_control<<<1, 1024, 0, stream_>>>(d_qd_, d_ctl_, ns, d_rd_, d_pre_);
-      if (prof) CK(cudaEventRecord(pe[3 * r], stream_));
-      k_light<<<light_grid, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
-      if (prof) CK(cudaEventRecord(pe[3 * r + 1], stream_));
-      k_heavy<<<heavy_grid, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
-      if (prof) CK(cudaEventRecord(pe[3 * r + 2], stream_));
+    if (round_graph_ && R == rounds_per_sync_ && !prof) {
+      CK(cudaGraphLaunch(round_graph_, stream_));
+    } else {
+      // profiled blocks time every kernel with events between the launches
+      GraphDev gd{g_->d_beg, g_->d_adj, g_->V, g_->d_wcut};
+      const int ns = (int)nslots_hi_;
+      cudaEvent_t* pe = ev_prof_[h];
+      for (uint32_t r = 0; r < R; r++) {
+        k_control<<<1, 1024, 0, stream_>>>(d_qd_, d_ctl_, ns, d_rd_, d_pre_);
+        if (prof) CK(cudaEventRecord(pe[3 * r], stream_));
+        k_light<<<light_grid_, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
+        if (prof) CK(cudaEventRecord(pe[3 * r + 1], stream_));
+        k_heavy<<<heavy_grid_, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
+        if (prof) CK(cudaEventRecord(pe[3 * r + 2], stream_));
+      }
     }
+    const int ns = (int)nslots_hi_;
     CK(cudaGetLastError());
     prof_rounds_[h] = prof ? R : 0;
     g_->launches += 3ull * R;
@@ -722,6 +755,7 @@ class Runner {
   unsigned light_grid_ = 148 * 4, heavy_grid_ = 148 * 2;
   double last_call_ms_ = 0;
   double trace_ms_ = 0;
+  cudaGraphExec_t round_graph_ = nullptr;
 };
 
 // Copy a finished job into a caller result.

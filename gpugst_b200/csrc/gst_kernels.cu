@@ -1299,18 +1299,21 @@ __device__ __forceinline__ void decide(QDev& q, QCtl& c) {
 __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* __restrict__ ctl, int nslots,
                                                   RoundDesc* __restrict__ rd, uint32_t* __restrict__ pre) {
   __shared__ uint32_t wsum[32][NT];
-  __shared__ uint32_t live_cnt;
+  __shared__ uint32_t live_cnt, used_hi;
   const int tid = threadIdx.x;
   const uint32_t lane = tid & 31, wid = tid >> 5;
-  if (tid == 0) live_cnt = 0;
+  if (tid == 0) live_cnt = used_hi = 0;
   __syncthreads();
   uint32_t cnt[NT];
 #pragma unroll
   for (int t = 0; t < NT; t++) cnt[t] = 0;
-  if (tid < nslots) {
+  // the state alone first: most slots are free when the scan covers them all
+  const int32_t st0 = tid < nslots ? qd[tid].st : J_FREE;
+  if (st0 != J_FREE) atomicMax(&used_hi, (uint32_t)tid + 1u);
+  if (st0 != J_FREE && st0 != J_DONE) {
     QDev q = qd[tid];
     QCtl& c = ctl[tid];
-    if (q.st != J_FREE && q.st != J_DONE) {
+    {
       absorb(q, c);
       if (q.st != J_DONE) decide(q, c);
       switch (q.act) {
@@ -1383,6 +1386,7 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
     rd->task_off[NT] = off;
     rd->heavy_tasks = off;
     rd->n_live = live_cnt;
+    rd->nslots = used_hi;  // slots the round kernels search (all later ones are free)
     rd->n_big = 0;
     // hub chunking pays off only when the round is too small to fill the GPU
     rd->hub_on =
@@ -1403,6 +1407,7 @@ __global__ void __launch_bounds__(256, GSTB_LIGHT_MIN_BLOCKS) k_light(const QDev
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t ntasks = __ldcg(&rd->light_tasks);
+  nslots = min(nslots, (int)__ldcg(&rd->nslots));
   // prefixes over slots of the item types with many items, staged once per block
   __shared__ uint32_t s_pre[MAX_SLOTS + 1], s_dp[MAX_SLOTS + 1], s_hop[MAX_SLOTS + 1];
   __shared__ RelaxHdr s_hdr[8][SSSP_WMAX];
@@ -1478,6 +1483,7 @@ __global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, cons
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t nbig = rd->big ? min(__ldcg(&rd->n_big), rd->big_cap) : 0u;
   const uint32_t ntasks = __ldcg(&rd->heavy_tasks) + nbig;
+  nslots = min(nslots, (int)__ldcg(&rd->nslots));
   __shared__ uint32_t s_lb[MAX_SLOTS + 1];
   __shared__ RelaxHdr s_hub[8];
   __shared__ WarpStat s_ws[8];
