@@ -63,6 +63,9 @@ struct gst_graph {
   std::vector<uint32_t> grp_v;
   int device = 0;
   int num_sms = 148;
+  // launch parameters (defaults and GSTB_* overrides at creation, gst_tuning_set
+  // or gst_autotune later); every Runner of the graph reads them
+  gst_tuning tune{};
   // persistent round driver for gst_query / gst_query_batch (created lazily)
   void* runner = nullptr;
   std::mutex mu;
@@ -288,8 +291,8 @@ class Runner {
     CK(cudaEventCreateWithFlags(&ev_fin_, cudaEventDisableTiming));
     for (auto& hh : ev_prof_)
       for (auto& e : hh) CK(cudaEventCreate(&e));
-    delta_sssp_ = std::max(1u, env_u32("GSTB_DELTA_SSSP", 16));
-    delta_dp_ = std::max(1u, env_u32("GSTB_DELTA_DP", 8));
+    delta_sssp_ = g_->tune.delta_sssp;
+    delta_dp_ = g_->tune.delta_dp;
     cap_num_ = std::max(1u, env_u32("GSTB_SSSP_CAP_NUM", 1));
     cap_den_ = std::max(1u, env_u32("GSTB_SSSP_CAP_DEN", 2));
     max_edges_dev_ = env_u32("GSTB_MAX_TREE_EDGES", 1u << 16);
@@ -315,7 +318,7 @@ class Runner {
       memset(&rd, 0, sizeof(rd));
       rd.big = env_u32("GSTB_HUB_SPLIT", 1) ? d_big_ : nullptr;
       rd.big_cap = big_cap_;
-      rd.hub_min_deg = env_u32("GSTB_HUB_MIN_DEG", 256);
+      rd.hub_min_deg = g_->tune.hub_min_deg;
       rd.hub_min_rest = env_u32("GSTB_HUB_MIN_REST", 128);
       rd.hub_max_items = env_u32("GSTB_HUB_MAX_ITEMS", 1000000);
       rd.light_warps = light_grid_ * (256 / 32);
@@ -414,6 +417,16 @@ class Runner {
   bool has_free_slot() const { return n_used_ < max_slots_; }
   bool reserve(size_t bytes) { return arena_.reserve(bytes); }
   bool has_free(size_t bytes) const { return arena_.free_bytes() >= bytes; }
+
+  // Take the graph's launch parameters (between calls: nothing in flight).
+  gst_status apply_tuning() {
+    delta_sssp_ = g_->tune.delta_sssp;
+    delta_dp_ = g_->tune.delta_dp;
+    const uint32_t hub = g_->tune.hub_min_deg;
+    CK(cudaMemcpyAsync(&d_rd_->hub_min_deg, &hub, sizeof(hub), cudaMemcpyHostToDevice, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    return GST_OK;
+  }
   size_t live() const { return n_used_; }
 
   // Allocate the workspace, initialise it and install the job in a free
@@ -847,6 +860,9 @@ gst_status gst_graph_create(const uint32_t* beg_pos, const uint32_t* csr, const 
   gst_graph* g = new gst_graph();
   g->V = V;
   g->arcs = arcs;
+  g->tune.delta_sssp = std::max(1u, env_u32("GSTB_DELTA_SSSP", 16));
+  g->tune.delta_dp = std::max(1u, env_u32("GSTB_DELTA_DP", 8));
+  g->tune.hub_min_deg = std::max(32u, env_u32("GSTB_HUB_MIN_DEG", 256));
   cudaGetDevice(&g->device);
   cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device);
   if (cudaMalloc(&g->d_beg, (size_t)(V + 1) * 4) != cudaSuccess ||
@@ -952,6 +968,22 @@ gst_status gst_query(gst_graph* g, const uint32_t* groups, int k, int D, gst_res
   return (gst_status)st;
 }
 
+gst_status gst_tuning_get(gst_graph* g, gst_tuning* out) {
+  if (!g || !out) return GST_BAD_INPUT;
+  std::lock_guard<std::mutex> lock(g->mu);
+  *out = g->tune;
+  return GST_OK;
+}
+
+gst_status gst_tuning_set(gst_graph* g, const gst_tuning* t) {
+  if (!g || !t || t->delta_sssp < 1 || t->delta_dp < 1 || t->hub_min_deg < 32) return GST_BAD_INPUT;
+  std::lock_guard<std::mutex> lock(g->mu);
+  g->tune = *t;
+  g->tune.reserved = 0;
+  if (g->runner) return static_cast<Runner*>(g->runner)->apply_tuning();
+  return GST_OK;
+}
+
 gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const int32_t* ks, const int32_t* Ds,
                            gst_result* results, int32_t* statuses, int max_concurrent) {
   if (!g || n < 0 || (n > 0 && (!groups || !ks || !Ds || !statuses))) return GST_BAD_INPUT;
@@ -1051,6 +1083,67 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
       fprintf(stderr, "gstb: batch of %d: %.2f ms (prepare %.2f, run %.2f with %.2f on the device, results %.2f)\n", n,
               all, ms(t0, t1), ms(t1, t2), R.last_call_ms(), ms(t2, clk::now()));
   }
+  return GST_OK;
+}
+
+gst_status gst_autotune(gst_graph* g, int n, const uint32_t* groups, const int32_t* ks, const int32_t* Ds,
+                        int objective, gst_tuning* out) {
+  if (!g || n < 1 || !groups || !ks || !Ds || (objective != 0 && objective != 1)) return GST_BAD_INPUT;
+  std::vector<int32_t> statuses(n);
+  std::vector<uint32_t> edges;  // trees are not needed: results without edge buffers
+  std::vector<gst_result> res(n);
+  // time of the sample under the current tuning: the batch once (throughput)
+  // or every query alone (latency), best of two runs after a warm-up
+  auto measure = [&](double& ms) -> gst_status {
+    double bestv = 1e300;
+    for (int rep = 0; rep < 3; rep++) {
+      auto t0 = std::chrono::steady_clock::now();
+      if (objective == 0) {
+        for (auto& r : res) r = gst_result{};
+        gst_status st = gst_query_batch(g, n, groups, ks, Ds, res.data(), statuses.data(), 0);
+        if (st != GST_OK) return st;
+      } else {
+        for (int i = 0; i < n; i++) {
+          gst_result r{};
+          gst_status st = gst_query(g, groups + (size_t)i * GST_GROUPS_STRIDE, ks[i], Ds[i], &r);
+          if (st == GST_CUDA_ERROR || st == GST_INTERNAL) return st;
+        }
+      }
+      double t = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      if (rep > 0) bestv = std::min(bestv, t);
+    }
+    ms = bestv;
+    return GST_OK;
+  };
+  gst_tuning cur;
+  gst_status st = gst_tuning_get(g, &cur);
+  if (st != GST_OK) return st;
+  double best_ms = 0;
+  st = measure(best_ms);
+  if (st != GST_OK) return st;
+  // one parameter at a time over a few candidates each
+  const uint32_t cand_sssp[] = {8, 16, 32, 64};
+  const uint32_t cand_dp[] = {2, 4, 8, 16};
+  const uint32_t cand_hub[] = {128, 256, 512, 1024};
+  for (int param = 0; param < 3; param++) {
+    const uint32_t* cand = param == 0 ? cand_sssp : (param == 1 ? cand_dp : cand_hub);
+    for (int c = 0; c < 4; c++) {
+      gst_tuning t = cur;
+      uint32_t& field = param == 0 ? t.delta_sssp : (param == 1 ? t.delta_dp : t.hub_min_deg);
+      const uint32_t now = param == 0 ? cur.delta_sssp : (param == 1 ? cur.delta_dp : cur.hub_min_deg);
+      if (cand[c] == now) continue;
+      field = cand[c];
+      if ((st = gst_tuning_set(g, &t)) != GST_OK) return st;
+      double ms = 0;
+      if ((st = measure(ms)) != GST_OK) return st;
+      if (ms < best_ms * 0.98) {  // keep a change only if it is clearly faster
+        best_ms = ms;
+        cur = t;
+      }
+    }
+    if ((st = gst_tuning_set(g, &cur)) != GST_OK) return st;
+  }
+  if (out) *out = cur;
   return GST_OK;
 }
 
@@ -1335,8 +1428,8 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   q.far2_idx = 3;
   q.st = J_INIT;
   q.act = A_NONE;
-  q.delta_sssp = std::max(1u, env_u32("GSTB_DELTA_SSSP", 16));
-  q.delta_dp = std::max(1u, env_u32("GSTB_DELTA_DP", 8));
+  q.delta_sssp = g->tune.delta_sssp;
+  q.delta_dp = g->tune.delta_dp;
   QCtl c;
   memset(&c, 0, sizeof(c));
   c.best = INF32;

@@ -44,6 +44,11 @@ class GstError(RuntimeError):
         super().__init__(f"{what}: {STATUS_NAMES.get(status, status)}{detail}")
 
 
+class _Tuning(ctypes.Structure):
+    _fields_ = [("delta_sssp", ctypes.c_uint32), ("delta_dp", ctypes.c_uint32), ("hub_min_deg", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+
 class _Result(ctypes.Structure):
     _fields_ = [("cost", ctypes.c_int32), ("root", ctypes.c_uint32), ("n_edges", ctypes.c_int32),
                 ("max_edges", ctypes.c_int32), ("edges", ctypes.POINTER(ctypes.c_uint32)),
@@ -73,6 +78,9 @@ def lib():
         L.gst_status_string.restype = ctypes.c_char_p
         L.gst_last_cuda_error.restype = ctypes.c_char_p
         L.gst_last_cuda_error.argtypes = []
+        L.gst_tuning_get.argtypes = [vp, ctypes.POINTER(_Tuning)]
+        L.gst_tuning_set.argtypes = [vp, ctypes.POINTER(_Tuning)]
+        L.gst_autotune.argtypes = [vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, ctypes.POINTER(_Tuning)]
         L.gst_graph_num_vertices.restype = u32
         L.gst_graph_num_vertices.argtypes = [vp]
         L.gst_graph_num_arcs.restype = u64
@@ -180,6 +188,40 @@ class Engine:
         tot = np.zeros(NSTATS, dtype=np.uint64)
         lib().gst_profile_read(self._h, _ptr(ms), ctypes.byref(n), _ptr(tot))
         return float(ms[0]), float(ms[1]), n.value, {name: int(tot[i]) for i, name in enumerate(STAT_NAMES)}
+
+    def tuning(self) -> dict:
+        """The engine's launch parameters (gst_tuning_get)."""
+        t = _Tuning()
+        st = lib().gst_tuning_get(self._h, ctypes.byref(t))
+        if st != GST_OK:
+            raise GstError(st, "gst_tuning_get")
+        return {"delta_sssp": t.delta_sssp, "delta_dp": t.delta_dp, "hub_min_deg": t.hub_min_deg}
+
+    def set_tuning(self, **kw):
+        """Change launch parameters (gst_tuning_set); unnamed ones keep their values."""
+        cur = self.tuning()
+        cur.update(kw)
+        t = _Tuning(cur["delta_sssp"], cur["delta_dp"], cur["hub_min_deg"], 0)
+        st = lib().gst_tuning_set(self._h, ctypes.byref(t))
+        if st != GST_OK:
+            raise GstError(st, "gst_tuning_set")
+
+    def autotune(self, queries, Ds=None, objective: str = "throughput") -> dict:
+        """Pick launch parameters on a sample of queries (gst_autotune);
+        objective "throughput" (batches) or "latency" (one query at a time)."""
+        n = len(queries)
+        groups = np.zeros((n, GROUPS_STRIDE), dtype=np.uint32)
+        ks = np.zeros(n, dtype=np.int32)
+        for i, q in enumerate(queries):
+            ks[i] = len(q)
+            groups[i, :len(q)] = q
+        Darr = np.full(n, -1, dtype=np.int32) if Ds is None else np.ascontiguousarray(Ds, dtype=np.int32)
+        t = _Tuning()
+        st = lib().gst_autotune(self._h, n, _ptr(groups), _ptr(ks), _ptr(Darr),
+                                0 if objective == "throughput" else 1, ctypes.byref(t))
+        if st != GST_OK:
+            raise GstError(st, "gst_autotune")
+        return {"delta_sssp": t.delta_sssp, "delta_dp": t.delta_dp, "hub_min_deg": t.hub_min_deg}
 
     def query(self, groups, D: int = -1, max_edges: int = 4096) -> QueryResult:
         """One synchronous query (gst_query)."""

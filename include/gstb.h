@@ -139,6 +139,28 @@ gst_status gst_query(gst_graph* g, const uint32_t* groups, int k, int D, gst_res
 #define GST_NOALLOC_SCRATCH_BYTES (64ull << 20)
 gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, int k, int D, gst_result* out);
 
+/* Launch parameters of a graph's engine (no reference counterpart: the
+ * reference fixes its block sizes and thresholds at compile time, DPQ.cuh:43
+ * and GPUGST+/include/util.h:19-33).  Defaults, overridable at
+ * gst_graph_create by GSTB_DELTA_SSSP / GSTB_DELTA_DP / GSTB_HUB_MIN_DEG:
+ * 16, 8, 256.  None of them changes a result, only the work schedule. */
+typedef struct gst_tuning {
+  uint32_t delta_sssp;   /* width of the distance rounds' near-far window */
+  uint32_t delta_dp;     /* width of the DP rounds' near-far window */
+  uint32_t hub_min_deg;  /* a vertex with this many arcs to relax hands them out in chunks (>= 32) */
+  uint32_t reserved;
+} gst_tuning;
+
+gst_status gst_tuning_get(gst_graph* g, gst_tuning* out);
+gst_status gst_tuning_set(gst_graph* g, const gst_tuning* t);
+/* Autotuner for the graph's degree profile: times a sample of n queries
+ * (laid out as for gst_query_batch) under candidate settings, one parameter
+ * at a time, and keeps the fastest.  objective 0 = batch throughput
+ * (gst_query_batch), 1 = one query at a time (gst_query).  The chosen
+ * settings stay on the graph; out (may be null) receives them. */
+gst_status gst_autotune(gst_graph* g, int n, const uint32_t* groups, const int32_t* ks, const int32_t* Ds,
+                        int objective, gst_tuning* out);
+
 /* Row stride of the groups array of gst_query_batch. */
 #define GST_GROUPS_STRIDE 8
 

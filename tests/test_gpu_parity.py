@@ -220,3 +220,25 @@ def test_serve_alone_vs_in_the_mix(gst_lib, c1):
         assert got[i].status == a.status, (i, got[i].status, a.status)
         assert got[i].cost == a.cost, (i, got[i].cost, a.cost)
         assert got[i].latency_ms >= 0
+
+
+def test_autotune_keeps_results_exact(gst_lib, oracle_mod, c1):
+    """The autotuner only changes the work schedule: after tuning on a sample,
+    every cost still matches the oracle; explicit settings round-trip."""
+    eng, O = gst_lib, oracle_mod
+    g, gr, qs = c1
+    E = _engine(eng, g, gr)
+    sample = list(qs[3][:16])
+    t = E.autotune(sample, objective="throughput")
+    assert t["delta_sssp"] in (8, 16, 32, 64) and t["delta_dp"] in (2, 4, 8, 16)
+    assert t["hub_min_deg"] in (128, 256, 512, 1024)
+    assert E.tuning() == t
+    res = E.query_batch(list(qs[3][16:28]))
+    for q, r in zip(qs[3][16:28], res):
+        assert r.status == eng.GST_OK and r.cost == O.prunedpp(g, gr, q, 0).cost
+    E.set_tuning(delta_sssp=8, delta_dp=2, hub_min_deg=128)
+    assert E.tuning() == {"delta_sssp": 8, "delta_dp": 2, "hub_min_deg": 128}
+    for q in qs[3][28:32]:
+        r = E.query(q)
+        assert r.status == eng.GST_OK and r.cost == O.prunedpp(g, gr, q, 0).cost
+    E.close()
