@@ -293,8 +293,8 @@ class Runner {
       for (auto& e : hh) CK(cudaEventCreate(&e));
     delta_sssp_ = g_->tune.delta_sssp;
     delta_dp_ = g_->tune.delta_dp;
-    cap_num_ = std::max(1u, env_u32("GSTB_SSSP_CAP_NUM", 1));
-    cap_den_ = std::max(1u, env_u32("GSTB_SSSP_CAP_DEN", 2));
+    cap_num_ = g_->tune.cap_pct;
+    cap_den_ = 100;
     max_edges_dev_ = env_u32("GSTB_MAX_TREE_EDGES", 1u << 16);
     rounds_per_sync_ = std::min(64u, std::max(1u, env_u32("GSTB_ROUNDS_PER_SYNC", 4)));
     trace_ms_ = (double)env_u32("GSTB_TRACE_MS", 0);  // report host iterations slower than this
@@ -422,6 +422,8 @@ class Runner {
   gst_status apply_tuning() {
     delta_sssp_ = g_->tune.delta_sssp;
     delta_dp_ = g_->tune.delta_dp;
+    cap_num_ = g_->tune.cap_pct;
+    cap_den_ = 100;
     const uint32_t hub = g_->tune.hub_min_deg;
     CK(cudaMemcpyAsync(&d_rd_->hub_min_deg, &hub, sizeof(hub), cudaMemcpyHostToDevice, stream_));
     CK(cudaStreamSynchronize(stream_));
@@ -863,6 +865,7 @@ gst_status gst_graph_create(const uint32_t* beg_pos, const uint32_t* csr, const 
   g->tune.delta_sssp = std::max(1u, env_u32("GSTB_DELTA_SSSP", 16));
   g->tune.delta_dp = std::max(1u, env_u32("GSTB_DELTA_DP", 8));
   g->tune.hub_min_deg = std::max(32u, env_u32("GSTB_HUB_MIN_DEG", 256));
+  g->tune.cap_pct = std::min(100u, std::max(1u, env_u32("GSTB_SSSP_CAP_PCT", 60)));
   cudaGetDevice(&g->device);
   cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device);
   if (cudaMalloc(&g->d_beg, (size_t)(V + 1) * 4) != cudaSuccess ||
@@ -976,10 +979,11 @@ gst_status gst_tuning_get(gst_graph* g, gst_tuning* out) {
 }
 
 gst_status gst_tuning_set(gst_graph* g, const gst_tuning* t) {
-  if (!g || !t || t->delta_sssp < 1 || t->delta_dp < 1 || t->hub_min_deg < 32) return GST_BAD_INPUT;
+  if (!g || !t || t->delta_sssp < 1 || t->delta_dp < 1 || t->hub_min_deg < 32 || t->cap_pct < 1 ||
+      t->cap_pct > 100)
+    return GST_BAD_INPUT;
   std::lock_guard<std::mutex> lock(g->mu);
   g->tune = *t;
-  g->tune.reserved = 0;
   if (g->runner) return static_cast<Runner*>(g->runner)->apply_tuning();
   return GST_OK;
 }
@@ -1122,15 +1126,16 @@ gst_status gst_autotune(gst_graph* g, int n, const uint32_t* groups, const int32
   st = measure(best_ms);
   if (st != GST_OK) return st;
   // one parameter at a time over a few candidates each
-  const uint32_t cand_sssp[] = {8, 16, 32, 64};
-  const uint32_t cand_dp[] = {2, 4, 8, 16};
-  const uint32_t cand_hub[] = {128, 256, 512, 1024};
-  for (int param = 0; param < 3; param++) {
-    const uint32_t* cand = param == 0 ? cand_sssp : (param == 1 ? cand_dp : cand_hub);
+  const uint32_t cands[4][4] = {{50, 60, 67, 75}, {8, 16, 32, 64}, {2, 4, 8, 16}, {128, 256, 512, 1024}};
+  auto field_of = [](gst_tuning& t, int param) -> uint32_t& {
+    return param == 0 ? t.cap_pct : (param == 1 ? t.delta_sssp : (param == 2 ? t.delta_dp : t.hub_min_deg));
+  };
+  for (int param = 0; param < 4; param++) {
+    const uint32_t* cand = cands[param];
     for (int c = 0; c < 4; c++) {
       gst_tuning t = cur;
-      uint32_t& field = param == 0 ? t.delta_sssp : (param == 1 ? t.delta_dp : t.hub_min_deg);
-      const uint32_t now = param == 0 ? cur.delta_sssp : (param == 1 ? cur.delta_dp : cur.hub_min_deg);
+      uint32_t& field = field_of(t, param);
+      const uint32_t now = field_of(cur, param);
       if (cand[c] == now) continue;
       field = cand[c];
       if ((st = gst_tuning_set(g, &t)) != GST_OK) return st;
@@ -1420,8 +1425,8 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   q.full = (int)((1u << k) - 1u);
   q.WT = WT;
   q.phase = PH_SSSP;
-  q.cap_num = std::max(1u, env_u32("GSTB_SSSP_CAP_NUM", 1));
-  q.cap_den = std::max(1u, env_u32("GSTB_SSSP_CAP_DEN", 2));
+  q.cap_num = g->tune.cap_pct;
+  q.cap_den = 100;
   q.in_idx = 0;
   q.out_idx = 1;
   q.far_idx = 2;

@@ -46,7 +46,7 @@ class GstError(RuntimeError):
 
 class _Tuning(ctypes.Structure):
     _fields_ = [("delta_sssp", ctypes.c_uint32), ("delta_dp", ctypes.c_uint32), ("hub_min_deg", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("cap_pct", ctypes.c_uint32)]
 
 
 class _Result(ctypes.Structure):
@@ -195,13 +195,14 @@ class Engine:
         st = lib().gst_tuning_get(self._h, ctypes.byref(t))
         if st != GST_OK:
             raise GstError(st, "gst_tuning_get")
-        return {"delta_sssp": t.delta_sssp, "delta_dp": t.delta_dp, "hub_min_deg": t.hub_min_deg}
+        return {"delta_sssp": t.delta_sssp, "delta_dp": t.delta_dp, "hub_min_deg": t.hub_min_deg,
+                "cap_pct": t.cap_pct}
 
     def set_tuning(self, **kw):
         """Change launch parameters (gst_tuning_set); unnamed ones keep their values."""
         cur = self.tuning()
         cur.update(kw)
-        t = _Tuning(cur["delta_sssp"], cur["delta_dp"], cur["hub_min_deg"], 0)
+        t = _Tuning(cur["delta_sssp"], cur["delta_dp"], cur["hub_min_deg"], cur["cap_pct"])
         st = lib().gst_tuning_set(self._h, ctypes.byref(t))
         if st != GST_OK:
             raise GstError(st, "gst_tuning_set")
@@ -221,7 +222,8 @@ class Engine:
                                 0 if objective == "throughput" else 1, ctypes.byref(t))
         if st != GST_OK:
             raise GstError(st, "gst_autotune")
-        return {"delta_sssp": t.delta_sssp, "delta_dp": t.delta_dp, "hub_min_deg": t.hub_min_deg}
+        return {"delta_sssp": t.delta_sssp, "delta_dp": t.delta_dp, "hub_min_deg": t.hub_min_deg,
+                "cap_pct": t.cap_pct}
 
     def query(self, groups, D: int = -1, max_edges: int = 4096) -> QueryResult:
         """One synchronous query (gst_query)."""

@@ -142,20 +142,22 @@ gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, int k, int D,
 /* Launch parameters of a graph's engine (no reference counterpart: the
  * reference fixes its block sizes and thresholds at compile time, DPQ.cuh:43
  * and GPUGST+/include/util.h:19-33).  Defaults, overridable at
- * gst_graph_create by GSTB_DELTA_SSSP / GSTB_DELTA_DP / GSTB_HUB_MIN_DEG:
- * 16, 8, 256.  None of them changes a result, only the work schedule. */
+ * gst_graph_create by GSTB_DELTA_SSSP / GSTB_DELTA_DP / GSTB_HUB_MIN_DEG /
+ * GSTB_SSSP_CAP_PCT: 16, 8, 256, 60.  None of them changes a result, only the
+ * work schedule and how tight the lower bounds are. */
 typedef struct gst_tuning {
   uint32_t delta_sssp;   /* width of the distance rounds' near-far window */
   uint32_t delta_dp;     /* width of the DP rounds' near-far window */
   uint32_t hub_min_deg;  /* a vertex with this many arcs to relax hands them out in chunks (>= 32) */
-  uint32_t reserved;
+  uint32_t cap_pct;      /* distances are computed exactly up to this percentage of the incumbent (1..100) */
 } gst_tuning;
 
 gst_status gst_tuning_get(gst_graph* g, gst_tuning* out);
 gst_status gst_tuning_set(gst_graph* g, const gst_tuning* t);
 /* Autotuner for the graph's degree profile: times a sample of n queries
- * (laid out as for gst_query_batch) under candidate settings, one parameter
- * at a time, and keeps the fastest.  objective 0 = batch throughput
+ * (laid out as for gst_query_batch) under candidate settings (cap_pct 50/60/
+ * 67/75, delta_sssp 8..64, delta_dp 2..16, hub_min_deg 128..1024), one
+ * parameter at a time, and keeps the fastest.  objective 0 = batch throughput
  * (gst_query_batch), 1 = one query at a time (gst_query).  The chosen
  * settings stay on the graph; out (may be null) receives them. */
 gst_status gst_autotune(gst_graph* g, int n, const uint32_t* groups, const int32_t* ks, const int32_t* Ds,

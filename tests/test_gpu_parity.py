@@ -231,13 +231,13 @@ def test_autotune_keeps_results_exact(gst_lib, oracle_mod, c1):
     sample = list(qs[3][:16])
     t = E.autotune(sample, objective="throughput")
     assert t["delta_sssp"] in (8, 16, 32, 64) and t["delta_dp"] in (2, 4, 8, 16)
-    assert t["hub_min_deg"] in (128, 256, 512, 1024)
+    assert t["hub_min_deg"] in (128, 256, 512, 1024) and t["cap_pct"] in (50, 60, 67, 75)
     assert E.tuning() == t
     res = E.query_batch(list(qs[3][16:28]))
     for q, r in zip(qs[3][16:28], res):
         assert r.status == eng.GST_OK and r.cost == O.prunedpp(g, gr, q, 0).cost
-    E.set_tuning(delta_sssp=8, delta_dp=2, hub_min_deg=128)
-    assert E.tuning() == {"delta_sssp": 8, "delta_dp": 2, "hub_min_deg": 128}
+    E.set_tuning(delta_sssp=8, delta_dp=2, hub_min_deg=128, cap_pct=100)
+    assert E.tuning() == {"delta_sssp": 8, "delta_dp": 2, "hub_min_deg": 128, "cap_pct": 100}
     for q in qs[3][28:32]:
         r = E.query(q)
         assert r.status == eng.GST_OK and r.cost == O.prunedpp(g, gr, q, 0).cost
