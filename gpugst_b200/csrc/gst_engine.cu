@@ -191,6 +191,22 @@ class Arena {
 
 
  private:
+  // Give chunks that are entirely free back to the driver (a request larger
+  // than every free block can then get one allocation of its own).
+  void trim() {
+    for (auto it = chunks_.begin(); it != chunks_.end();) {
+      auto f = free_.find(it->first);
+      if (f != free_.end() && f->second == it->second) {
+        erase_free(f->first, f->second);
+        cudaFree(it->first);
+        held_ -= it->second;
+        it = chunks_.erase(it);
+      } else {
+        ++it;
+      }
+    }
+  }
+
   bool grow(size_t n, bool exact = false) {
     // chunks double from 64 MB up to GSTB_ARENA_MB (default 1 GB)
     const size_t step = (size_t)env_u32("GSTB_ARENA_MB", 1024) << 20;
@@ -201,7 +217,11 @@ class Arena {
       sz = n;
       if (cudaMalloc(&p, sz) != cudaSuccess) {
         cudaGetLastError();
-        return false;
+        trim();  // free chunks may be what the device is missing
+        if (cudaMalloc(&p, sz) != cudaSuccess) {
+          cudaGetLastError();
+          return false;
+        }
       }
     }
     chunks_[static_cast<char*>(p)] = sz;
