@@ -19,6 +19,9 @@
 //   qbuf   u32 [4][cap]        near-in, near-out, far, far-out work lists of state ids
 //   tour   u32 [k][2^k][k] + [k][2^k] + [8][8]  tour tables P, T2 and group distances
 //   lbt    u16 [V][2^k]        lower bound of completing (v, X) to every group
+//   snap   u32 [D-1][V][8]     hop-bounded queries: the distance rows after
+//                               Bellman-Ford round b (b = 1..D-1), i.e. lower
+//                               bounds of the cheapest paths of at most b hops
 #pragma once
 #include <cstdint>
 
@@ -43,7 +46,7 @@ enum Action : int32_t { A_NONE = 0, A_SSEED, A_WORK, A_SPLIT, A_TOUR, A_LB, A_DS
 // Task types of one round.  Light kernel: split, seeds, tour, extract,
 // distance items and DP states; heavy kernel: the arc chunks the light kernel
 // handed over, then lower-bound table rows.
-enum TaskType : int32_t { T_SPLIT = 0, T_SSEED, T_DSEED, T_TOUR, T_EXTRACT, T_SSSP, T_DP, T_HOP, T_LB, NT };
+enum TaskType : int32_t { T_SPLIT = 0, T_SSEED, T_DSEED, T_TOUR, T_EXTRACT, T_SSSP, T_DP, T_HOP, T_LB, T_SNAP, NT };
 constexpr int MAX_SLOTS = 1024;
 
 // Round-wide work description written by k_control.
@@ -148,7 +151,10 @@ struct QDev {
   uint32_t par;      // parity of the items in (or entering) the near list
   uint32_t lb_off;   // bound-table rows (vertices) already computed
   uint32_t hops;     // distance rounds done (hop-bounded queries stop after D)
-  uint32_t pad_h;
+  uint32_t snap_h;   // distance round whose rows k_heavy copies to snap this round (0: none)
+  uint32_t snap_n;   // snapshots taken (rows for b hops: snap[b-1] if b <= snap_n, else dist)
+  uint32_t pad_s;
+  uint32_t* snap;    // [D-1][V][8] (hop-bounded queries)
 };
 
 struct GraphDev {

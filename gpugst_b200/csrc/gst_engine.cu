@@ -261,7 +261,7 @@ class Arena {
 
 // Workspace layout of one query (see gst_device.cuh).
 struct Layout {
-  size_t table, dist, dflag, qbuf, tour, lbt, members, edges, total;
+  size_t table, dist, dflag, qbuf, tour, lbt, snap, members, edges, total;
   uint32_t cap;
 };
 
@@ -286,6 +286,8 @@ Layout layout_for(const gst_graph* g, int k, int nd, size_t n_members, uint32_t 
   L.qbuf = o; o = align_up(o + 4 * cap * 4, 256);
   L.tour = o; o = align_up(o + ((size_t)k * (1u << k) * k + (size_t)k * (1u << k) + 64) * 4, 256);
   L.lbt = o; o = align_up(o + (size_t)g->V * (1u << k) * 2, 256);
+  // hop-bounded queries: distance rows after Bellman-Ford rounds 1..D-1
+  L.snap = o; o = align_up(o + (nd >= 3 ? (size_t)(nd - 2) * g->V * ROW * 4 : 0), 256);
   L.members = o; o = align_up(o + std::max<size_t>(n_members, 1) * 4, 256);
   L.edges = o; o = align_up(o + (size_t)std::max<uint32_t>(max_edges, 1) * 12, 256);
   L.total = o;
@@ -477,6 +479,7 @@ class Runner {
     for (int b = 0; b < 4; b++) q.qbuf[b] = (uint32_t*)(j->mem + L.qbuf) + (size_t)b * L.cap;
     q.tour = (uint32_t*)(j->mem + L.tour);
     q.lbt = (unsigned short*)(j->mem + L.lbt);
+    q.snap = (uint32_t*)(j->mem + L.snap);
     q.nv = g_->V;
     q.members = (const uint32_t*)(j->mem + L.members);
     q.out_edges = (uint32_t*)(j->mem + L.edges);
@@ -1432,6 +1435,7 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   for (int b = 0; b < 4; b++) q.qbuf[b] = (uint32_t*)(ws + L.qbuf) + (size_t)b * L.cap;
   q.tour = (uint32_t*)(ws + L.tour);
   q.lbt = (unsigned short*)(ws + L.lbt);
+  q.snap = (uint32_t*)(ws + L.snap);
   q.members = (const uint32_t*)(ws + L.members);
   q.out_edges = (uint32_t*)(ws + L.edges);
   q.ctl = d_ctl;

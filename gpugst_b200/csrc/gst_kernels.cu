@@ -442,6 +442,28 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
   }
 }
 
+// Hop-bounded queries: lower bound of joining every group of comp to v
+// within b hops, INF32 if one is out of reach.  In a derivation of a tree of
+// hop diameter <= D from state (v, p, d), a group missing from p is reached
+// from v by a path outside the subtree, and that path plus the subtree's
+// height d is a path of the tree: it has at most D - d hops.  Rows for b hops
+// are the snapshot after Bellman-Ford round b (or the final rows once the
+// rounds stopped); for b = 0 only v itself counts (distance 0: v is in the
+// group).  Every lane calls it; lanes j < k read word j of the row.
+__device__ __forceinline__ uint32_t hop_budget_lb(const QDev& q, uint32_t v, uint32_t comp, uint32_t b,
+                                                  uint32_t lane) {
+  const uint32_t* row = (b >= 1u && b <= q.snap_n) ? q.snap + ((size_t)(b - 1u) * q.nv + v) * ROW
+                                                   : q.dist + (size_t)v * ROW;
+  uint32_t x = 0;
+  if (lane < (uint32_t)q.k && ((comp >> lane) & 1u)) {
+    x = __ldcg(row + lane);
+    if (b == 0u) x = x == 0u ? 0u : INF32;
+  }
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) x = max(x, __shfl_xor_sync(0xFFFFFFFFu, x, o));
+  return __shfl_sync(0xFFFFFFFFu, x, 0);
+}
+
 // ---------------------------------------------------------------------------
 // Hop-bounded DP item (v, p, d): state id ((v << k) | p) * nd + d.
 // ---------------------------------------------------------------------------
@@ -468,6 +490,11 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
     return;
   }
   const uint32_t comp = full ^ p;
+  {
+    // the missing groups within the hops left (D - d) of v
+    const uint32_t lbh = hop_budget_lb(q, v, comp, (uint32_t)D - d, lane);
+    if (lbh == INF32 || (unsigned long long)c + lbh > best) return;
+  }
   if (lane == 0) ws_add(ws, q.ctl, ST_EXPANDED, 1u);
   const unsigned short* lbt = q.lbt;
   uint32_t lbv = __ldg(lbt + ((size_t)v << k) + comp);
@@ -1166,6 +1193,7 @@ __device__ __forceinline__ void absorb(QDev& q, QCtl& c) {
     return;
   }
   int t;
+  q.snap_h = 0;  // a snapshot scheduled last round has been copied
   switch (q.act) {
     case A_SSEED:
       t = q.in_idx; q.in_idx = q.out_idx; q.out_idx = t;
@@ -1178,7 +1206,13 @@ __device__ __forceinline__ void absorb(QDev& q, QCtl& c) {
       q.n_in = c.n_near;
       q.n_far = c.n_far;
       q.par ^= 1u;  // producers of the round flagged the next items with the other parity
-      if (q.st == J_SSSP) q.hops++;
+      if (q.st == J_SSSP) {
+        q.hops++;
+        // rows after round b bound the paths of at most b hops: copy them
+        // while the next round runs (a value it lowers in the meantime is
+        // still a valid bound)
+        if (q.D >= 0 && q.hops < (uint32_t)q.D) q.snap_h = q.hops;
+      }
       break;
     case A_SPLIT:
       t = q.in_idx; q.in_idx = q.out_idx; q.out_idx = t;
@@ -1235,6 +1269,7 @@ __device__ __forceinline__ void decide(QDev& q, QCtl& c) {
           // final tree has at most D hops, so these are valid lower bounds,
           // and an unreached vertex cannot join a group
           q.cap1 = BIG;
+          q.snap_n = min(q.hops, (uint32_t)q.D - 1u);
           q.st = J_TOUR;
           continue;
         }
@@ -1258,6 +1293,9 @@ __device__ __forceinline__ void decide(QDev& q, QCtl& c) {
           return;
         }
         if (q.st == J_SSSP) {
+          // a hop-bounded query whose rounds converged before D: rows for
+          // more hops than the snapshots taken are the final distances
+          if (q.D >= 0) q.snap_n = min(q.hops, q.D > 0 ? (uint32_t)q.D - 1u : 0u);
           // every distance below theta_hi is exact and every distance <=
           // cap(best) was discovered; unknown ones are >= min(theta_hi, cap+1)
           unsigned long long b1 = c.best == INF32 ? (unsigned long long)INF32 : limit + 1;
@@ -1328,6 +1366,7 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
           break;
         default: break;
       }
+      if (q.snap_h) cnt[T_SNAP] = q.nv;  // copy the distance rows of round snap_h
       if (q.st != J_DONE) atomicAdd(&live_cnt, 1u);
       qd[tid] = q;
     }
@@ -1371,7 +1410,7 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
     const unsigned long long n_sssp = wsum[(blockDim.x >> 5) - 1][T_SSSP];
     while (w < SSSP_WMAX && n_sssp > 2ull * w * rd->light_warps) w <<= 1;
     rd->sssp_w = w;
-    const uint32_t per_task[NT] = {32, 32, 32, 1, 1, w, 1, 1, 4};
+    const uint32_t per_task[NT] = {32, 32, 32, 1, 1, w, 1, 1, 4, 32};
     uint32_t off = 0;
     for (int t = 0; t < NT; t++) {
       uint32_t tot = wsum[(blockDim.x >> 5) - 1][t];
@@ -1476,7 +1515,7 @@ __global__ void __launch_bounds__(256, GSTB_LIGHT_MIN_BLOCKS) k_light(const QDev
 // Heavy round kernel: the arc chunks k_light handed over this round (hub
 // vertices of distance items, high-degree DP states), then lower-bound table
 // rows (8 lanes per vertex).
-__global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, const RoundDesc* __restrict__ rd,
+__global__ void __launch_bounds__(256, 3) k_heavy(const QDev* __restrict__ qd, const RoundDesc* __restrict__ rd,
                                                const uint32_t* __restrict__ pre, int nslots, GraphDev g) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1496,7 +1535,8 @@ __global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, cons
   }
   for (int i = threadIdx.x; i <= nslots; i += blockDim.x) s_lb[i] = __ldcg(pre + T_LB * (MAX_SLOTS + 1) + i);
   __syncthreads();
-  const uint32_t n_lb = __ldcg(&rd->items[T_LB]);
+  const uint32_t n_lb = __ldcg(&rd->items[T_LB]), n_snap = __ldcg(&rd->items[T_SNAP]);
+  const uint32_t snap0 = __ldcg(&rd->task_off[T_SNAP]);  // heavy tasks before the snapshot rows
   for (uint32_t task = warp; task < ntasks; task += nwarps) {
     if (task < nbig) {
       const uint4 it = __ldcg(rd->big + task);
@@ -1506,11 +1546,28 @@ __global__ void __launch_bounds__(256) k_heavy(const QDev* __restrict__ qd, cons
         hub_chunk(qd, it, g, lane, &s_hub[threadIdx.x >> 5], ws, wb);
       continue;
     }
-    const uint32_t it = (task - nbig) * 4u + (lane >> 3);
-    if (it < n_lb) {
-      const uint32_t slot = find_slot_s(s_lb, nslots, it);
-      const QDev& ql = qd[slot];
-      lbt_row8(ql, ql.lb_off + (it - s_lb[slot]), lane & 7u);
+    const uint32_t ht = task - nbig;
+    if (ht < snap0) {  // lower-bound table rows, 8 lanes per vertex
+      const uint32_t it = ht * 4u + (lane >> 3);
+      if (it < n_lb) {
+        const uint32_t slot = find_slot_s(s_lb, nslots, it);
+        const QDev& ql = qd[slot];
+        lbt_row8(ql, ql.lb_off + (it - s_lb[slot]), lane & 7u);
+      }
+      continue;
+    }
+    // snapshot of a hop-bounded query's distance rows, one row per lane
+    const uint32_t it = (ht - snap0) * 32u + lane;
+    if (it < n_snap) {
+      const uint32_t* P = pre + T_SNAP * (MAX_SLOTS + 1);
+      const uint32_t slot = find_slot(P, nslots, it);
+      const QDev& qs = qd[slot];
+      const uint32_t v = it - __ldcg(P + slot);
+      const uint4* src = reinterpret_cast<const uint4*>(qs.dist + (size_t)v * ROW);
+      uint4* dst = reinterpret_cast<uint4*>(qs.snap + ((size_t)(qs.snap_h - 1u) * qs.nv + v) * ROW);
+      const uint4 a = __ldcg(src), b = __ldcg(src + 1);
+      dst[0] = a;
+      dst[1] = b;
     }
   }
   wb_flush(wb, lane);
