@@ -63,6 +63,7 @@ struct gst_graph {
   std::vector<uint32_t> grp_v;
   int device = 0;
   int num_sms = 148;
+  size_t total_mem = 0;  // the device's memory (bytes)
   // launch parameters (defaults and GSTB_* overrides at creation, gst_tuning_set
   // or gst_autotune later); every Runner of the graph reads them
   gst_tuning tune{};
@@ -179,6 +180,11 @@ class Arena {
   }
 
   size_t free_bytes() const { return free_total_; }
+  // Give back every wholly free chunk when more than `keep` bytes are held
+  // (after a batch, so that its memory does not starve other engines).
+  void release_above(size_t keep) {
+    if (held_ > keep) trim();
+  }
 
   void release() {
     for (auto& c : chunks_) cudaFree(c.first);
@@ -439,6 +445,7 @@ class Runner {
   bool has_free_slot() const { return n_used_ < max_slots_; }
   bool reserve(size_t bytes) { return arena_.reserve(bytes); }
   bool has_free(size_t bytes) const { return arena_.free_bytes() >= bytes; }
+  void release_arena_above(size_t keep) { arena_.release_above(keep); }
 
   // Take the graph's launch parameters (between calls: nothing in flight).
   gst_status apply_tuning() {
@@ -891,6 +898,13 @@ gst_status gst_graph_create(const uint32_t* beg_pos, const uint32_t* csr, const 
   g->tune.cap_pct = std::min(100u, std::max(1u, env_u32("GSTB_SSSP_CAP_PCT", 60)));
   cudaGetDevice(&g->device);
   cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device);
+  {
+    size_t fr = 0;
+    if (cudaMemGetInfo(&fr, &g->total_mem) != cudaSuccess) {
+      cudaGetLastError();
+      g->total_mem = 0;
+    }
+  }
   if (cudaMalloc(&g->d_beg, (size_t)(V + 1) * 4) != cudaSuccess ||
       cudaMalloc(&g->d_adj, std::max<size_t>(arcs, 1) * 8) != cudaSuccess) {
     cudaGetLastError();
@@ -1093,6 +1107,13 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
       },
       [&](Job*) {});
   if (rs != GST_OK) return rs;
+  // a large batch's workspaces go back to the device (serving loops and
+  // other engines allocate their own) once the arena holds more than
+  // GSTB_ARENA_KEEP_MB, by default a quarter of the device's memory
+  {
+    const uint32_t keep_mb = env_u32("GSTB_ARENA_KEEP_MB", 0);
+    R.release_arena_above(keep_mb ? (size_t)keep_mb << 20 : g->total_mem / 4);
+  }
   const clk::time_point t2 = clk::now();
   for (int i = 0; i < n; i++) {
     Job& j = jobs[i];
