@@ -506,11 +506,39 @@ struct PrunedDP {
   }
 };
 
+// Cheapest path from group j to v with at most b hops, b = 0..D (synchronous
+// Bellman-Ford rounds), as hd[(b * k + j) * V + v]; HD_INF if none.
+const int32_t HD_INF = 0x3FFFFFFF;
+std::vector<int32_t> hop_limited_distances(const Csr& g, const Query& q, int D) {
+  const size_t V = g.V;
+  std::vector<int32_t> hd((size_t)(D + 1) * q.k * V, HD_INF);
+  for (int j = 0; j < q.k; j++)
+    for (uint32_t m : q.groups[j]) hd[(size_t)j * V + m] = 0;
+  for (int b = 1; b <= D; b++)
+    for (int j = 0; j < q.k; j++) {
+      const int32_t* prev = &hd[((size_t)(b - 1) * q.k + j) * V];
+      int32_t* cur = &hd[((size_t)b * q.k + j) * V];
+      std::copy(prev, prev + V, cur);
+      for (uint32_t u = 0; u < g.V; u++) {
+        if (prev[u] >= HD_INF) continue;
+        for (uint32_t a = g.beg[u]; a < g.beg[u + 1]; a++)
+          cur[g.adj[a]] = std::min(cur[g.adj[a]], prev[u] + g.w[a]);
+      }
+    }
+  return hd;
+}
+
 // ---------------------------------------------------------------------------
-// HOP_cpu restatement (CPUHOP.h:107-288)
+// HOP_cpu restatement (CPUHOP.h:107-288).  With `hd` (the hop-limited
+// distances) it also applies the GPU engine's hop-budget bound at pop time,
+// against the upper bound `ub`: a state (v, p, d) is dropped when a group
+// missing from p has no member within D - d hops of v, or when its cost plus
+// the largest such distance exceeds ub.  This variant is test infrastructure
+// for that bound's exactness.
 // ---------------------------------------------------------------------------
 int run_hop(const Csr& g, const Query& q, int D, int32_t* cost_out, uint32_t* root_out,
-            int32_t* n_edges, uint32_t* edges, int max_edges, int64_t* stats) {
+            int32_t* n_edges, uint32_t* edges, int max_edges, int64_t* stats,
+            const std::vector<int32_t>* hd = nullptr, int64_t ub = INT64_MAX) {
   int k = q.k, W_ = 1 << k, full = W_ - 1, DD = D + 1;
   size_t NS = (size_t)g.V * W_ * DD;
   std::vector<TNode> t(NS, TNode{INF, 0, 0, 0, 0, 0, 0});
@@ -543,6 +571,18 @@ int run_hop(const Csr& g, const Query& q, int D, int32_t* cost_out, uint32_t* ro
       fin = e;
       found = true;
       break;
+    }
+    if (hd) {
+      int64_t lb = 0;
+      bool reach = true;
+      const int b = D - e.d;
+      for (int j = 0; j < k; j++)
+        if (!((e.p >> j) & 1)) {
+          const int32_t x = (*hd)[((size_t)b * k + j) * g.V + e.v];
+          if (x >= HD_INF) reach = false;
+          lb = std::max<int64_t>(lb, x);
+        }
+      if (!reach || e.cost + lb > ub) continue;
     }
     if (e.d < D) {
       for (uint32_t a = g.beg[e.v]; a < g.beg[e.v + 1]; a++) {
@@ -739,6 +779,19 @@ int oracle_hop(uint32_t V, const uint32_t* beg, const uint32_t* adj, const int32
   Csr g{V, beg, adj, w};
   Query q = make_query(g, k, qptr, qv);
   return run_hop(g, q, D, cost, root, n_edges, edges, max_edges, stats);
+}
+
+// HOP_cpu with the hop-budget bound against the upper bound ub (see run_hop).
+int oracle_hop_budget(uint32_t V, const uint32_t* beg, const uint32_t* adj, const int32_t* w, int k,
+                      const uint64_t* qptr, const uint32_t* qv, int D, int64_t ub, int32_t* cost,
+                      int64_t* stats) {
+  if (k < 1 || k > 14 || D < 0) return 2;
+  Csr g{V, beg, adj, w};
+  Query q = make_query(g, k, qptr, qv);
+  std::vector<int32_t> hd = hop_limited_distances(g, q, D);
+  uint32_t root = 0;
+  int32_t ne = 0;
+  return run_hop(g, q, D, cost, &root, &ne, nullptr, 0, stats, &hd, ub);
 }
 
 int oracle_dpbf(uint32_t V, const uint32_t* beg, const uint32_t* adj, const int32_t* w, int k,

@@ -32,7 +32,8 @@ def lib():
             build()
         _lib = ctypes.CDLL(LIB)
         P = ctypes.c_void_p
-        for name in ("oracle_prunedpp", "oracle_hop", "oracle_dpbf", "oracle_brute", "oracle_validate"):
+        for name in ("oracle_prunedpp", "oracle_hop", "oracle_hop_budget", "oracle_dpbf", "oracle_brute",
+                     "oracle_validate"):
             getattr(_lib, name).restype = ctypes.c_int
     return _lib
 
@@ -81,6 +82,18 @@ def prunedpp(graph, groups, query, ratio: int = 0) -> Result:
 
 def hop(graph, groups, query, D: int) -> Result:
     return _run(lib().oracle_hop, graph, groups, query, (ctypes.c_int(D),))
+
+
+def hop_budget(graph, groups, query, D: int, ub: int):
+    """HOP_cpu with the engine's hop-budget bound against the upper bound ub:
+    (status, cost, states popped)."""
+    ptr, qv = _query_arrays(groups, query)
+    cost = ctypes.c_int32(0)
+    stats = np.zeros(4, dtype=np.int64)
+    st = lib().oracle_hop_budget(ctypes.c_uint32(graph.V), _p(graph.beg_pos), _p(graph.csr), _p(graph.weight),
+                                 ctypes.c_int(len(query)), _p(ptr), _p(qv), ctypes.c_int(D), ctypes.c_int64(ub),
+                                 ctypes.byref(cost), _p(stats))
+    return st, cost.value, int(stats[0])
 
 
 def dpbf(graph, groups, query) -> Result:

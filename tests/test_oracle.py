@@ -3,7 +3,7 @@ import numpy as np
 import pytest
 
 from gpugst_b200 import gen
-from tests.cases import tiny_cases
+from tests.cases import small_cases, tiny_cases
 
 
 def test_generators_shape():
@@ -76,3 +76,27 @@ def test_validator_rejects(oracle_mod):
         bad = r.edges.copy()
         bad[0, 2] += 1
         assert O.validate(g, gr, q, -1, r.cost, r.root, bad) == 1
+
+
+def test_hop_budget_bound_keeps_the_optimum(oracle_mod):
+    """The hop-budget bound the engine applies to hop-bounded DP states: a
+    state (v, S, d) may be dropped when a group missing from S has no member
+    within D - d hops of v, or when its cost plus the largest such distance
+    exceeds an upper bound.  Applied with the optimum itself as the upper
+    bound (the tightest the engine ever has), HOP_cpu must still reach the
+    optimum, and must still find no tree where there is none."""
+    O = oracle_mod
+    checked = pruned_any = 0
+    for i, (g, gr, q) in enumerate(small_cases(30, seed0=700, V=150, E=500, kmax=5)):
+        for D in (0, 1, 2, 3, 4):
+            ref = O.hop(g, gr, q, D)
+            ub = ref.cost if ref.status == 0 else 1 << 40
+            st, cost, popped = O.hop_budget(g, gr, q, D, ub)
+            if ref.status != 0:
+                assert st != 0, (i, D)
+                continue
+            assert st == 0 and cost == ref.cost, (i, D, ref.cost, st, cost)
+            checked += 1
+            pruned_any += popped < ref.process
+    assert checked >= 50
+    assert pruned_any > 0  # the bound does cut states on these instances
