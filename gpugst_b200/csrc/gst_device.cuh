@@ -117,7 +117,10 @@ struct alignas(64) QCtl {
   uint32_t status;   // extraction: 0 ok, 1 no solution, 2 cycle / inconsistency
   uint32_t done;     // job finished (set by k_control)
   uint32_t final_status;  // gst_status of the finished job
-  uint32_t pad2[4];
+  uint32_t cancel;   // set by the host: end the job at the next round (GST_CANCELLED)
+  uint32_t early;    // progressive mode: the DP stopped early (1) ...
+  uint32_t lb_exit;  // ... with this lower bound on the optimum proven
+  uint32_t pad2[1];
 };
 
 // Per-query descriptor; the host rewrites it before each round.
@@ -155,6 +158,9 @@ struct QDev {
   uint32_t snap_n;   // snapshots taken (rows for b hops: snap[b-1] if b <= snap_n, else dist)
   uint32_t pad_s;
   uint32_t* snap;    // [D-1][V][8] (hop-bounded queries)
+  // progressive mode: return the best recorded tree once its cost is at most
+  // ratio_num / ratio_den times the proven lower bound (ratio_num 0: exact)
+  uint32_t ratio_num, ratio_den;
 };
 
 struct GraphDev {

@@ -14,15 +14,19 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <map>
 #include <mutex>
+#include <shared_mutex>
 #include <thread>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "../../include/gstb.h"
@@ -58,9 +62,12 @@ struct gst_graph {
   uint32_t* d_beg = nullptr;
   uint2* d_adj = nullptr;
   uint32_t* d_wcut = nullptr;  // per vertex: first arc with weight > 2^b, b = 0..7
-  // group index (host copy; member lists of a query are built on the host)
+  // group index (host copy; member lists of a query are built on the host).
+  // gst_groups_set replaces it under grp_mu held exclusively; every reader
+  // (query preparation in all entry points) holds it shared
   std::vector<uint64_t> grp_ptr;
   std::vector<uint32_t> grp_v;
+  std::shared_mutex grp_mu;
   int device = 0;
   int num_sms = 148;
   size_t total_mem = 0;  // the device's memory (bytes)
@@ -71,6 +78,8 @@ struct gst_graph {
   void* runner = nullptr;
   std::mutex mu;
   std::atomic<uint64_t> launches{0};
+  // fault injection (gst_debug_fail_allocs): workspace allocations still to fail
+  std::atomic<int> fail_allocs{0};
   bool profile = false;
   double prof_light_ms = 0, prof_heavy_ms = 0;
   uint64_t prof_rounds = 0;
@@ -78,6 +87,11 @@ struct gst_graph {
 };
 
 namespace {
+
+bool has_groups(gst_graph* g) {
+  std::shared_lock<std::shared_mutex> lock(g->grp_mu);
+  return !g->grp_ptr.empty();
+}
 
 uint32_t env_u32(const char* name, uint32_t def) {
   const char* s = getenv(name);
@@ -90,6 +104,7 @@ struct Job {
   uint32_t groups[KMAX];
   int k = 0, D = -1;
   uint64_t tag = 0;
+  uint32_t ratio_num = 0;     // progressive mode: ratio * 1024 (0: exact)
   gst_result* res = nullptr;  // caller result (may be null: serve copies out)
   // derived
   int nd = 1;
@@ -106,7 +121,10 @@ struct Job {
   uint32_t retries = 0;      // runs repeated after GST_QUEUE_OVERFLOW
   gst_status status = GST_OK;
   bool rejected = false;  // failed validation before admission
+  bool cancelled = false; // withdrawn while waiting for a rerun
   bool done = false;
+  bool early_done = false;   // fill_result has settled the progressive answer
+  uint32_t lower_bound = 0;  // proven lower bound on the optimum
   // results
   int32_t cost = -1;
   uint32_t root = 0;
@@ -115,6 +133,46 @@ struct Job {
 };
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Progressive-mode ratios are rationals num / RATIO_DEN.
+constexpr uint32_t RATIO_DEN = 1024;
+uint32_t ratio_to_num(double ratio) {
+  if (!(ratio > 1.0)) return 0;  // exact (also NaN)
+  return (uint32_t)std::floor(std::min(ratio, 1.0e6) * RATIO_DEN);  // rounded down: never looser than asked
+}
+
+// Minimum spanning forest (Kruskal) of an edge multiset given as (u, v, w)
+// triples; duplicates collapse.  A progressive answer's derivation may reuse
+// edges across subtrees or close cycles (its sub-states can have been lowered
+// after it was recorded); its edges stay connected, so the spanning tree
+// covers the same vertices, hence the same groups, at no greater cost (the
+// reference post-processes its incumbent the same way,
+// graph_hash_of_mixed_weighted_MST_postprocessing_no_whole_graph).
+void spanning_tree(std::vector<uint32_t>& e) {
+  const size_t n = e.size() / 3;
+  std::vector<size_t> ord(n);
+  for (size_t i = 0; i < n; i++) ord[i] = i;
+  std::sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return e[3 * a + 2] < e[3 * b + 2]; });
+  std::unordered_map<uint32_t, uint32_t> id;
+  std::vector<uint32_t> par;
+  auto node = [&](uint32_t v) {
+    auto it = id.find(v);
+    if (it != id.end()) return it->second;
+    uint32_t x = (uint32_t)par.size();
+    id[v] = x;
+    par.push_back(x);
+    return x;
+  };
+  std::function<uint32_t(uint32_t)> find = [&](uint32_t x) { return par[x] == x ? x : par[x] = find(par[x]); };
+  std::vector<uint32_t> out;
+  for (size_t i : ord) {
+    uint32_t a = find(node(e[3 * i])), b = find(node(e[3 * i + 1]));
+    if (a == b) continue;
+    par[a] = b;
+    out.insert(out.end(), {e[3 * i], e[3 * i + 1], e[3 * i + 2]});
+  }
+  e.swap(out);
+}
 
 // Device workspace arena of one Runner: chunks from cudaMalloc, carved by
 // best fit with coalescing.  Admission never waits on the driver's allocator
@@ -126,7 +184,17 @@ class Arena {
  public:
   ~Arena() { release(); }
 
+  // Counter of injected failures (gst_debug_fail_allocs): while it is
+  // positive, each workspace allocation fails as if the device were full.
+  void set_fail_counter(std::atomic<int>* c) { fail_ = c; }
+
   void* alloc(size_t n) {
+    if (fail_) {
+      int f = fail_->load();
+      while (f > 0 && !fail_->compare_exchange_weak(f, f - 1)) {
+      }
+      if (f > 0) return nullptr;
+    }
     n = align_up(std::max<size_t>(n, 1), 256);
     auto it = by_size_.lower_bound(n);
     if (it == by_size_.end()) {
@@ -263,6 +331,7 @@ class Arena {
   std::multimap<size_t, char*> by_size_;  // size -> free block
   std::unordered_map<char*, size_t> used_;
   size_t held_ = 0, in_use_ = 0, free_total_ = 0;
+  std::atomic<int>* fail_ = nullptr;
 };
 
 // Workspace layout of one query (see gst_device.cuh).
@@ -312,6 +381,7 @@ class Runner {
   ~Runner() { release(); }
 
   gst_status init() {
+    arena_.set_fail_counter(&g_->fail_allocs);
     CK(cudaSetDevice(g_->device));
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     for (auto& e : ev_) CK(cudaEventCreate(&e));
@@ -359,6 +429,8 @@ class Runner {
     CK(cudaMallocHost(&h_ctl_, 2 * MAX_SLOTS * sizeof(QCtl)));
     CK(cudaMallocHost(&h_rd_, sizeof(RoundDesc)));
     CK(cudaMallocHost(&h_qd_, sizeof(QDev)));
+    CK(cudaMallocHost(&h_one_, sizeof(uint32_t)));
+    *h_one_ = 1u;
     // pinned staging for admissions (descriptors + member lists) and for the
     // tree read-back of retired jobs: copies from pinned memory stay
     // asynchronous, pageable ones would synchronise the stream each time
@@ -388,6 +460,8 @@ class Runner {
     if (h_ctl_) cudaFreeHost(h_ctl_);
     if (h_rd_) cudaFreeHost(h_rd_);
     if (h_qd_) cudaFreeHost(h_qd_);
+    if (h_one_) cudaFreeHost(h_one_);
+    h_one_ = nullptr;
     if (h_stage_) cudaFreeHost(h_stage_);
     if (h_edge_stage_) cudaFreeHost(h_edge_stage_);
     h_stage_ = nullptr;
@@ -419,7 +493,9 @@ class Runner {
   gst_status prepare(Job* j) {
     if (j->k < 1 || j->k > KMAX) return GST_BAD_INPUT;
     if (j->D > DMAX) return GST_BAD_INPUT;
-    const uint32_t ng = (uint32_t)(g_->grp_ptr.empty() ? 0 : g_->grp_ptr.size() - 1);
+    std::shared_lock<std::shared_mutex> glock(g_->grp_mu);
+    if (g_->grp_ptr.empty()) return GST_BAD_INPUT;
+    const uint32_t ng = (uint32_t)(g_->grp_ptr.size() - 1);
     for (int i = 0; i < j->k; i++)
       if (j->groups[i] >= ng) return GST_BAD_INPUT;
     for (int a = 0; a < j->k; a++)
@@ -510,6 +586,8 @@ class Runner {
     q.act = A_NONE;
     q.delta_sssp = delta_sssp_;
     q.delta_dp = delta_dp_;
+    q.ratio_num = j->D < 0 ? j->ratio_num : 0u;
+    q.ratio_den = RATIO_DEN;
     memset(&j->ctl, 0, sizeof(j->ctl));
     j->ctl.best = INF32;
     j->ctl.best_full = INF64;
@@ -543,6 +621,30 @@ class Runner {
     j->mem = nullptr;
   }
 
+  // Withdraw the admitted job with this tag: its control block's cancel flag
+  // is set stream-ordered after the block in flight, and k_control ends the
+  // job at its next round with GST_CANCELLED.  False if no admitted job has
+  // the tag (the caller checks its pending queue).
+  bool cancel_tag(uint64_t tag) {
+    for (Job* j : retry_)
+      if (j->tag == tag) {
+        j->cancelled = true;  // reported as cancelled instead of being rerun
+        return true;
+      }
+    for (uint32_t s = 0; s < slots_.size(); s++) {
+      Job* j = slots_[s];
+      if (j && j->tag == tag) {
+        if (cudaMemcpyAsync(&d_ctl_[s].cancel, h_one_, sizeof(uint32_t), cudaMemcpyHostToDevice, stream_) !=
+            cudaSuccess) {
+          last_cuda_error() = cudaGetLastError();
+          return false;
+        }
+        return true;
+      }
+    }
+    return false;
+  }
+
   double last_call_ms() const { return last_call_ms_; }
   double trace_ms() const { return trace_ms_; }
 
@@ -571,6 +673,14 @@ class Runner {
       // queries retried with larger frontier lists go first
       while (!retry_.empty() && has_free_slot()) {
         Job* j = retry_.front();
+        if (j->cancelled) {
+          j->status = GST_CANCELLED;
+          j->done = true;
+          j->t_done = std::chrono::steady_clock::now();
+          retry_.pop_front();
+          on_done(j);
+          continue;
+        }
         if (!admit(j)) {
           if (n_used_ > 0) break;  // wait for memory
           j->status = GST_OOM;     // does not fit even alone
@@ -787,6 +897,7 @@ class Runner {
   QCtl* h_ctl_ = nullptr;
   RoundDesc* h_rd_ = nullptr;
   QDev* h_qd_ = nullptr;
+  uint32_t* h_one_ = nullptr;  // pinned 1, the source of cancel flags
   char* h_stage_ = nullptr;
   char* h_edge_stage_ = nullptr;
   size_t stage_cap_ = 0, stage_off_[2] = {0, 0}, edge_stage_cap_ = 0;
@@ -806,11 +917,27 @@ class Runner {
 // Copy a finished job into a caller result.
 gst_status fill_result(Job* j, gst_result* r) {
   if (!r) return j->status;
+  // a progressive answer: its derivation's edges reduced to a spanning tree
+  // (once: poll and batch results call this once per job)
+  if (j->status == GST_OK && j->ctl.early && j->edges.size() / 3 == j->ctl.n_edges) {
+    spanning_tree(j->edges);
+    int64_t sum = 0;
+    for (size_t e = 0; e < j->edges.size() / 3; e++) sum += j->edges[3 * e + 2];
+    j->cost = (int32_t)sum;
+    j->ctl.n_edges = (uint32_t)(j->edges.size() / 3);
+    j->ctl.early = 0;
+    j->ctl.lb_exit = std::min<uint32_t>(j->ctl.lb_exit, (uint32_t)sum);
+    j->lower_bound = j->ctl.lb_exit;
+  } else if (j->status == GST_OK && !j->early_done) {
+    j->lower_bound = (uint32_t)j->cost;
+  }
+  j->early_done = true;
   r->cost = j->status == GST_OK ? j->cost : -1;
   r->root = j->root;
-  for (int i = 0; i < GST_NSTATS; i++) r->stats[i] = j->ctl.stat[i];
+  for (int i = 0; i < 12; i++) r->stats[i] = j->ctl.stat[i];
   r->stats[GST_STAT_TABLE_BYTES] = j->table_bytes;
   r->stats[GST_STAT_RETRIES] = j->retries;
+  r->stats[GST_STAT_LOWER_BOUND] = j->status == GST_OK ? j->lower_bound : 0;
   r->latency_ms = std::chrono::duration<double, std::milli>(j->t_done - j->t_submit).count();
   gst_status st = j->status;
   if (st == GST_OK) {
@@ -854,6 +981,7 @@ const char* gst_status_string(gst_status st) {
     case GST_BUSY: return "busy";
     case GST_NOT_FOUND: return "not found";
     case GST_SCRATCH_TOO_SMALL: return "query workspace exceeds the static scratch";
+    case GST_CANCELLED: return "cancelled";
   }
   return "unknown";
 }
@@ -889,6 +1017,24 @@ gst_status gst_graph_create(const uint32_t* beg_pos, const uint32_t* csr, const 
   for (auto& x : th) x.join();
   bad = abad;
   if (bad) return GST_BAD_INPUT;
+  // Integer range: every distance and tree cost is summed in 32 bits and the
+  // lower bounds saturate at BIG = 2^30 (a saturated bound reads as
+  // "unreachable").  A shortest path or a tree has at most V-1 edges, so the
+  // V-1 heaviest arcs bound every such cost; the graph is rejected if that
+  // bound can reach 2^30.
+  if (arcs) {
+    uint32_t wmax = 0;
+    for (uint64_t a = 0; a < arcs; a++) wmax = std::max(wmax, adj[a].y);
+    if ((uint64_t)(V - 1) * wmax >= (uint64_t)BIG) {
+      std::vector<uint32_t> ws(arcs);
+      for (uint64_t a = 0; a < arcs; a++) ws[a] = adj[a].y;
+      const size_t m = std::min<size_t>(ws.size(), (size_t)V - 1);
+      std::nth_element(ws.begin(), ws.begin() + m, ws.end(), std::greater<uint32_t>());
+      uint64_t heavy = 0;
+      for (size_t i = 0; i < m; i++) heavy += ws[i];
+      if (heavy >= (uint64_t)BIG) return GST_BAD_INPUT;
+    }
+  }
   gst_graph* g = new gst_graph();
   g->V = V;
   g->arcs = arcs;
@@ -956,6 +1102,7 @@ gst_status gst_groups_set(gst_graph* g, const uint64_t* grp_ptr, const uint32_t*
   if (n && !grp_v) return GST_BAD_INPUT;
   for (uint64_t t = 0; t < n; t++)
     if (grp_v[t] >= g->V) return GST_BAD_INPUT;
+  std::unique_lock<std::shared_mutex> lock(g->grp_mu);
   g->grp_ptr.assign(grp_ptr, grp_ptr + n_groups + 1);
   g->grp_v.assign(grp_v, grp_v + n);
   return GST_OK;
@@ -997,15 +1144,19 @@ void gst_profile_reset(gst_graph* g) {
 uint32_t gst_graph_num_vertices(const gst_graph* g) { return g ? g->V : 0; }
 uint64_t gst_graph_num_arcs(const gst_graph* g) { return g ? g->arcs : 0; }
 
-gst_status gst_query(gst_graph* g, const uint32_t* groups, int k, int D, gst_result* out) {
+gst_status gst_query_ratio(gst_graph* g, const uint32_t* groups, int k, int D, double ratio, gst_result* out) {
   int32_t ks = k, Ds = D;
   int32_t st = 0;
   if (k < 1 || k > KMAX || !groups) return GST_BAD_INPUT;
-  uint32_t gg[KMAX] = {0};
+  uint32_t gg[GST_GROUPS_STRIDE] = {0};
   memcpy(gg, groups, (size_t)k * 4);
-  gst_status s = gst_query_batch(g, 1, gg, &ks, &Ds, out, &st, 1);
+  gst_status s = gst_query_batch_ratio(g, 1, gg, &ks, &Ds, &ratio, out, &st, 1);
   if (s != GST_OK) return s;
   return (gst_status)st;
+}
+
+gst_status gst_query(gst_graph* g, const uint32_t* groups, int k, int D, gst_result* out) {
+  return gst_query_ratio(g, groups, k, D, 0.0, out);
 }
 
 gst_status gst_tuning_get(gst_graph* g, gst_tuning* out) {
@@ -1027,8 +1178,13 @@ gst_status gst_tuning_set(gst_graph* g, const gst_tuning* t) {
 
 gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const int32_t* ks, const int32_t* Ds,
                            gst_result* results, int32_t* statuses, int max_concurrent) {
+  return gst_query_batch_ratio(g, n, groups, ks, Ds, nullptr, results, statuses, max_concurrent);
+}
+
+gst_status gst_query_batch_ratio(gst_graph* g, int n, const uint32_t* groups, const int32_t* ks, const int32_t* Ds,
+                                 const double* ratios, gst_result* results, int32_t* statuses, int max_concurrent) {
   if (!g || n < 0 || (n > 0 && (!groups || !ks || !Ds || !statuses))) return GST_BAD_INPUT;
-  if (g->grp_ptr.empty()) return GST_BAD_INPUT;
+  if (!has_groups(g)) return GST_BAD_INPUT;
   std::lock_guard<std::mutex> lock(g->mu);
   if (!g->runner) {
     Runner* nr = new Runner(g);
@@ -1049,6 +1205,7 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
     j.k = ks[i];
     j.D = Ds[i] < 0 ? -1 : Ds[i];
     j.tag = (uint64_t)i;
+    j.ratio_num = ratios ? ratio_to_num(ratios[i]) : 0u;
     j.res = results ? &results[i] : nullptr;
     if (j.k < 1 || j.k > KMAX) {
       statuses[i] = GST_BAD_INPUT;
@@ -1121,7 +1278,7 @@ gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const in
     statuses[i] = fill_result(&j, j.res);
     if (j.res) j.res->device_ms = R.last_call_ms();
     if (g->profile)
-      for (int t = 0; t < GST_NSTATS; t++) g->prof_stats[t] += j.ctl.stat[t];
+      for (int t = 0; t < 12; t++) g->prof_stats[t] += j.ctl.stat[t];
   }
   const double tr = R.trace_ms();
   if (tr > 0) {
@@ -1215,6 +1372,9 @@ struct gst_server {
   uint64_t budget = 0, in_use = 0;
   size_t max_inflight = 0, inflight = 0;
   size_t max_pending = 1u << 20;
+  std::vector<uint64_t> cancels;  // admitted requests to withdraw (the loop applies them)
+  std::unordered_multiset<uint64_t> running;  // ids of the admitted requests
+  uint64_t n_submitted = 0, n_completed = 0, n_busy = 0, n_cancelled = 0, n_oom = 0;
   gst_status fatal = GST_OK;
 };
 
@@ -1229,6 +1389,8 @@ static void serve_loop(gst_server* S) {
     gst_status st = S->runner->run(
         [&]() {
           std::lock_guard<std::mutex> lk(S->mu);
+          for (uint64_t id : S->cancels) S->runner->cancel_tag(id);
+          S->cancels.clear();
           while (!S->pending.empty() && S->inflight < S->max_inflight && S->runner->has_free_slot()) {
             Job* j = S->pending.front();
             if (S->in_use + j->bytes > S->budget && S->inflight > 0) break;  // wait for memory
@@ -1239,6 +1401,8 @@ static void serve_loop(gst_server* S) {
                 j->t_done = std::chrono::steady_clock::now();
                 S->pending.pop_front();
                 S->finished.push_back(j);
+                S->n_completed++;
+                S->n_oom++;
                 continue;
               }
               break;
@@ -1246,13 +1410,21 @@ static void serve_loop(gst_server* S) {
             S->pending.pop_front();
             S->inflight++;
             S->in_use += j->bytes;
+            S->running.insert(j->tag);
           }
         },
         [&](Job* j) {
           std::lock_guard<std::mutex> lk(S->mu);
           S->inflight--;
           S->in_use -= j->bytes;
+          {
+            auto it = S->running.find(j->tag);
+            if (it != S->running.end()) S->running.erase(it);
+          }
           S->finished.push_back(j);
+          S->n_completed++;
+          if (j->status == GST_CANCELLED) S->n_cancelled++;
+          if (j->status == GST_OOM) S->n_oom++;
         });
     if (st != GST_OK) {
       std::lock_guard<std::mutex> lk(S->mu);
@@ -1265,7 +1437,7 @@ static void serve_loop(gst_server* S) {
 extern "C" {
 
 gst_status gst_serve_open(gst_graph* g, uint64_t hbm_budget_bytes, int max_inflight, gst_server** out) {
-  if (!g || !out || g->grp_ptr.empty()) return GST_BAD_INPUT;
+  if (!g || !out || !has_groups(g)) return GST_BAD_INPUT;
   *out = nullptr;
   gst_server* S = new gst_server();
   S->g = g;
@@ -1291,9 +1463,15 @@ gst_status gst_serve_open(gst_graph* g, uint64_t hbm_budget_bytes, int max_infli
 }
 
 gst_status gst_serve_submit(gst_server* S, uint64_t req_id, const uint32_t* groups, int k, int D) {
+  return gst_serve_submit_ratio(S, req_id, groups, k, D, 0.0);
+}
+
+gst_status gst_serve_submit_ratio(gst_server* S, uint64_t req_id, const uint32_t* groups, int k, int D,
+                                  double ratio) {
   if (!S || !groups) return GST_BAD_INPUT;
   Job* j = new Job();
   j->tag = req_id;
+  j->ratio_num = ratio_to_num(ratio);
   j->k = k;
   j->D = D < 0 ? -1 : D;
   j->t_submit = std::chrono::steady_clock::now();
@@ -1313,12 +1491,16 @@ gst_status gst_serve_submit(gst_server* S, uint64_t req_id, const uint32_t* grou
     j->done = true;
     j->t_done = j->t_submit;
     S->finished.push_back(j);
+    S->n_submitted++;
+    S->n_completed++;
     return GST_OK;
   }
   if (S->pending.size() >= S->max_pending) {
     delete j;
+    S->n_busy++;
     return GST_BUSY;
   }
+  S->n_submitted++;
   S->pending.push_back(j);
   S->cv.notify_one();
   return GST_OK;
@@ -1355,6 +1537,58 @@ gst_status gst_serve_poll(gst_server* S, uint64_t* ids, int32_t* statuses, gst_r
     delete j;
   }
   *n_out = (int)got.size();
+  return GST_OK;
+}
+
+gst_status gst_serve_cancel(gst_server* S, uint64_t req_id) {
+  if (!S) return GST_BAD_INPUT;
+  std::lock_guard<std::mutex> lk(S->mu);
+  for (auto it = S->pending.begin(); it != S->pending.end(); ++it) {
+    Job* j = *it;
+    if (j->tag != req_id) continue;
+    S->pending.erase(it);  // never admitted: finished at once
+    j->status = GST_CANCELLED;
+    j->rejected = true;
+    j->done = true;
+    j->t_done = std::chrono::steady_clock::now();
+    S->finished.push_back(j);
+    S->n_completed++;
+    S->n_cancelled++;
+    return GST_OK;
+  }
+  if (S->running.find(req_id) == S->running.end()) return GST_NOT_FOUND;
+  // admitted: the serving loop withdraws it at its next iteration (a request
+  // that finishes meanwhile keeps its own result)
+  S->cancels.push_back(req_id);
+  return GST_OK;
+}
+
+gst_status gst_serve_set_max_pending(gst_server* S, uint64_t max_pending) {
+  if (!S || max_pending == 0) return GST_BAD_INPUT;
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->max_pending = (size_t)max_pending;
+  return GST_OK;
+}
+
+gst_status gst_serve_stats(gst_server* S, gst_serve_info* out) {
+  if (!S || !out) return GST_BAD_INPUT;
+  std::lock_guard<std::mutex> lk(S->mu);
+  out->pending = S->pending.size();
+  out->inflight = S->inflight;
+  out->finished_unpolled = S->finished.size();
+  out->budget_bytes = S->budget;
+  out->in_use_bytes = S->in_use;
+  out->submitted = S->n_submitted;
+  out->completed = S->n_completed;
+  out->rejected_busy = S->n_busy;
+  out->cancelled = S->n_cancelled;
+  out->oom = S->n_oom;
+  return GST_OK;
+}
+
+gst_status gst_debug_fail_allocs(gst_graph* g, int n) {
+  if (!g || n < 0) return GST_BAD_INPUT;
+  g->fail_allocs.store(n);
   return GST_OK;
 }
 
@@ -1398,28 +1632,33 @@ struct DeviceGuard {
 
 extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, int k, int D, gst_result* out) {
   if (!g || !groups || k < 1 || k > KMAX || D > DMAX) return GST_BAD_INPUT;
-  if (g->grp_ptr.empty()) return GST_BAD_INPUT;
   if (D < 0) D = -1;
-  const uint32_t ng = (uint32_t)(g->grp_ptr.size() - 1);
-  for (int i = 0; i < k; i++)
-    if (groups[i] >= ng) return GST_BAD_INPUT;
   for (int a = 0; a < k; a++)
     for (int b = a + 1; b < k; b++)
       if (groups[a] == groups[b]) return GST_BAD_INPUT;
   const int nd = D < 0 ? 1 : D + 1;
   const uint32_t WT = (1u << k) * (uint32_t)nd;
-  if ((uint64_t)g->V * WT >= (1ull << 32)) return GST_BAD_INPUT;
+  // the same size limits as the other entry points (member items are v*8+j in 32 bits)
+  if ((uint64_t)g->V * WT >= (1ull << 32) || g->V >= (1u << 29)) return GST_BAD_INPUT;
+  if (g->device < 0 || g->device >= NOALLOC_MAX_DEVICES) return GST_BAD_INPUT;
+  // the graph's lock first (the group index and the tuning are read below and
+  // gst_groups_set / gst_tuning_set change them under it), then the scratch's
+  std::lock_guard<std::mutex> glock(g->mu);
+  std::shared_lock<std::shared_mutex> grlock(g->grp_mu);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g->grp_ptr.empty()) return GST_BAD_INPUT;
+  const uint32_t ng = (uint32_t)(g->grp_ptr.size() - 1);
+  for (int i = 0; i < k; i++)
+    if (groups[i] >= ng) return GST_BAD_INPUT;
   uint64_t n_members = 0;
   for (int i = 0; i < k; i++) {
     uint64_t n = g->grp_ptr[groups[i] + 1] - g->grp_ptr[groups[i]];
     if (n == 0) return GST_NO_SOLUTION;
     n_members += n;
   }
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
   DeviceGuard guard;
   CK(cudaGetDevice(&guard.prev));
   CK(cudaSetDevice(g->device));
-  if (g->device < 0 || g->device >= NOALLOC_MAX_DEVICES) return GST_BAD_INPUT;
   if (!g_noalloc_base[g->device]) {
     void* p = nullptr;
     CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
@@ -1504,14 +1743,15 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
     rd0.sssp_w = 4;
     CK(cudaMemcpy(d_rd, &rd0, sizeof(RoundDesc), cudaMemcpyHostToDevice));
   }
-  // member items v*8 + j, staged through a fixed host buffer
+  // member items v*8 + j, staged through a fixed host array (calls are
+  // serialised, so one array serves them all): one copy per 64K members
   {
-    uint32_t stage[1024];
+    static uint32_t stage[1u << 16];
     size_t n = 0, off = 0;
     for (int i = 0; i < k; i++) {
       for (uint64_t t = g->grp_ptr[groups[i]]; t < g->grp_ptr[groups[i] + 1]; t++) {
         stage[n++] = g->grp_v[t] * 8u + (uint32_t)i;
-        if (n == 1024) {
+        if (n == (1u << 16)) {
           CK(cudaMemcpy((uint32_t*)q.members + off, stage, n * 4, cudaMemcpyHostToDevice));
           off += n;
           n = 0;
@@ -1546,8 +1786,10 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
     out->cost = st == GST_OK ? (int32_t)(c.best_full >> 32) : -1;
     out->root = c.root;
     out->n_edges = st == GST_OK ? (int32_t)c.n_edges : 0;
-    for (int i = 0; i < GST_NSTATS; i++) out->stats[i] = c.stat[i];
+    for (int i = 0; i < 12; i++) out->stats[i] = c.stat[i];
     out->stats[GST_STAT_TABLE_BYTES] = (uint64_t)g->V * WT * 8;
+    out->stats[GST_STAT_RETRIES] = 0;
+    out->stats[GST_STAT_LOWER_BOUND] = st == GST_OK ? (uint64_t)(c.best_full >> 32) : 0;
     out->device_ms = out->latency_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     if (st == GST_OK) {
       uint32_t ne = std::min<uint32_t>(c.n_edges, max_edges);

@@ -1186,6 +1186,12 @@ __device__ void extract_one(const QDev& q, const GraphDev& g) {
 // exclusive prefix sums over slots (pre[t][0..nslots]).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void absorb(QDev& q, QCtl& c) {
+  if (c.cancel) {  // the host withdrew the request
+    q.st = J_DONE;
+    c.final_status = 12;  // GST_CANCELLED
+    c.done = 1;
+    return;
+  }
   if (c.overflow) {
     q.st = J_DONE;
     c.final_status = 6;  // GST_QUEUE_OVERFLOW
@@ -1272,6 +1278,22 @@ __device__ __forceinline__ void decide(QDev& q, QCtl& c) {
           q.snap_n = min(q.hops, (uint32_t)q.D - 1u);
           q.st = J_TOUR;
           continue;
+        }
+        if (q.st == J_DP && q.phase == PH_DP && q.ratio_num != 0u && c.best_full != INF64) {
+          // Progressive exit (CPUNONHOP.h:730-755, in exact integer
+          // arithmetic).  Every state of cost below lo (theta_lo, or theta_hi
+          // once the window's near list is empty) has been expanded at its
+          // final cost.  The optimum's derivation has no state costlier than
+          // the optimum, so an optimum below lo would already be recorded:
+          // opt >= min(best_full, lo).  Stop once best_full <= ratio * lo.
+          const unsigned long long lo = q.n_in > 0 ? q.theta_lo : q.theta_hi;
+          const unsigned long long bf = c.best_full >> 32;
+          if (bf * q.ratio_den <= lo * q.ratio_num) {
+            c.early = 1u;
+            c.lb_exit = (uint32_t)(bf < lo ? bf : lo);
+            q.st = J_EXTRACT;
+            continue;
+          }
         }
         if (q.n_in > 0) {
           c.n_near = 0;

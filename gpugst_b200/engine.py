@@ -25,11 +25,12 @@ LIB_PATH = os.path.join(HERE, "libgstb.so")
 GST_OK, GST_NO_SOLUTION, GST_BAD_INPUT, GST_OOM = 0, 1, 2, 3
 GST_DEVICE_TIMEOUT, GST_CUDA_ERROR, GST_QUEUE_OVERFLOW, GST_TRUNCATED = 4, 5, 6, 7
 GST_INTERNAL, GST_BUSY, GST_NOT_FOUND, GST_SCRATCH_TOO_SMALL = 8, 9, 10, 11
+GST_CANCELLED = 12
 STATUS_NAMES = {0: "ok", 1: "no solution", 2: "bad input", 3: "out of memory", 4: "device timeout",
                 5: "cuda error", 6: "queue overflow", 7: "truncated", 8: "internal", 9: "busy",
-                10: "not found", 11: "scratch too small"}
+                10: "not found", 11: "scratch too small", 12: "cancelled"}
 STAT_NAMES = ["expanded", "sssp_items", "arcs", "updates", "enqueued", "rounds", "merges", "table_bytes",
-              "sssp_arcs", "sssp_updates", "sssp_enqueued", "retries"]
+              "sssp_arcs", "sssp_updates", "sssp_enqueued", "retries", "lower_bound"]
 NSTATS = len(STAT_NAMES)
 GROUPS_STRIDE = 8  # row stride of gst_query_batch's groups array
 KMAX = 7           # query groups at most
@@ -49,10 +50,16 @@ class _Tuning(ctypes.Structure):
                 ("cap_pct", ctypes.c_uint32)]
 
 
+class _ServeInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("pending", "inflight", "finished_unpolled", "budget_bytes",
+                                               "in_use_bytes", "submitted", "completed", "rejected_busy",
+                                               "cancelled", "oom")]
+
+
 class _Result(ctypes.Structure):
     _fields_ = [("cost", ctypes.c_int32), ("root", ctypes.c_uint32), ("n_edges", ctypes.c_int32),
                 ("max_edges", ctypes.c_int32), ("edges", ctypes.POINTER(ctypes.c_uint32)),
-                ("stats", ctypes.c_uint64 * 12), ("device_ms", ctypes.c_double),
+                ("stats", ctypes.c_uint64 * NSTATS), ("device_ms", ctypes.c_double),
                 ("latency_ms", ctypes.c_double)]
 
 
@@ -73,6 +80,9 @@ def lib():
         L.gst_graph_destroy.restype = None
         L.gst_query.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Result)]
         L.gst_query_batch.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_int]
+        L.gst_query_batch_ratio.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, vp, ctypes.c_int]
+        L.gst_query_ratio.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(_Result)]
+        L.gst_serve_submit_ratio.argtypes = [vp, u64, vp, ctypes.c_int, ctypes.c_int, ctypes.c_double]
         L.gst_query_noalloc.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Result)]
         L.gst_query_noalloc.restype = ctypes.c_int
         L.gst_status_string.restype = ctypes.c_char_p
@@ -97,9 +107,15 @@ def lib():
         L.gst_serve_submit.argtypes = [vp, u64, vp, ctypes.c_int, ctypes.c_int]
         L.gst_serve_poll.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
         L.gst_serve_close.argtypes = [vp]
-        for name in ("gst_serve_open", "gst_serve_submit", "gst_serve_poll", "gst_serve_close"):
+        L.gst_serve_cancel.argtypes = [vp, u64]
+        L.gst_serve_set_max_pending.argtypes = [vp, u64]
+        L.gst_serve_stats.argtypes = [vp, ctypes.POINTER(_ServeInfo)]
+        L.gst_debug_fail_allocs.argtypes = [vp, ctypes.c_int]
+        for name in ("gst_serve_open", "gst_serve_submit", "gst_serve_poll", "gst_serve_close", "gst_serve_cancel",
+                     "gst_serve_set_max_pending", "gst_serve_stats", "gst_debug_fail_allocs"):
             getattr(L, name).restype = ctypes.c_int
-        for name in ("gst_graph_create", "gst_groups_set", "gst_query", "gst_query_batch"):
+        for name in ("gst_graph_create", "gst_groups_set", "gst_query", "gst_query_batch", "gst_query_batch_ratio",
+                     "gst_query_ratio", "gst_serve_submit_ratio"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -172,6 +188,12 @@ class Engine:
         stats = {name: int(r.stats[i]) for i, name in enumerate(STAT_NAMES)}
         return QueryResult(st, r.cost, r.root, edges, stats, r.device_ms, r.latency_ms)
 
+    def fail_allocs(self, n: int):
+        """Fault injection: the next n workspace allocations fail (gst_debug_fail_allocs)."""
+        st = lib().gst_debug_fail_allocs(self._h, int(n))
+        if st != GST_OK:
+            raise GstError(st, "gst_debug_fail_allocs")
+
     def kernel_launches(self) -> int:
         return int(lib().gst_kernel_launches(self._h))
 
@@ -225,14 +247,18 @@ class Engine:
         return {"delta_sssp": t.delta_sssp, "delta_dp": t.delta_dp, "hub_min_deg": t.hub_min_deg,
                 "cap_pct": t.cap_pct}
 
-    def query(self, groups, D: int = -1, max_edges: int = 4096) -> QueryResult:
-        """One synchronous query (gst_query)."""
+    def query(self, groups, D: int = -1, max_edges: int = 4096, ratio: float = 0.0) -> QueryResult:
+        """One synchronous query (gst_query; gst_query_ratio when ratio > 1:
+        progressive mode, cost at most ratio x the optimum)."""
         g = np.ascontiguousarray(groups, dtype=np.uint32)
         buf = np.zeros(3 * max_edges, dtype=np.uint32)
         r = _Result()
         r.max_edges = max_edges
         r.edges = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
-        st = lib().gst_query(self._h, _ptr(g), len(g), int(D), ctypes.byref(r))
+        if ratio:
+            st = lib().gst_query_ratio(self._h, _ptr(g), len(g), int(D), float(ratio), ctypes.byref(r))
+        else:
+            st = lib().gst_query(self._h, _ptr(g), len(g), int(D), ctypes.byref(r))
         if st in (GST_CUDA_ERROR, GST_INTERNAL):
             raise GstError(st, "gst_query")
         return self._unpack(st, r, buf)
@@ -250,8 +276,9 @@ class Engine:
             raise GstError(st, "gst_query_noalloc")
         return self._unpack(st, r, buf)
 
-    def query_batch(self, queries, Ds=None, max_concurrent: int = 0, max_edges: int = 4096):
-        """Many queries sharing device rounds (gst_query_batch)."""
+    def query_batch(self, queries, Ds=None, max_concurrent: int = 0, max_edges: int = 4096, ratios=None):
+        """Many queries sharing device rounds (gst_query_batch; per-query
+        progressive-mode ratios through gst_query_batch_ratio)."""
         n = len(queries)
         groups = np.zeros((n, GROUPS_STRIDE), dtype=np.uint32)
         ks = np.zeros(n, dtype=np.int32)
@@ -267,8 +294,13 @@ class Engine:
             bufs.append(b)
             res[i].max_edges = max_edges
             res[i].edges = b.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
-        st = lib().gst_query_batch(self._h, n, _ptr(groups), _ptr(ks), _ptr(Darr), ctypes.cast(res, ctypes.c_void_p), _ptr(statuses),
-                                   int(max_concurrent))
+        if ratios is None:
+            st = lib().gst_query_batch(self._h, n, _ptr(groups), _ptr(ks), _ptr(Darr), ctypes.cast(res, ctypes.c_void_p),
+                                       _ptr(statuses), int(max_concurrent))
+        else:
+            rat = np.ascontiguousarray(ratios, dtype=np.float64)
+            st = lib().gst_query_batch_ratio(self._h, n, _ptr(groups), _ptr(ks), _ptr(Darr), _ptr(rat),
+                                             ctypes.cast(res, ctypes.c_void_p), _ptr(statuses), int(max_concurrent))
         if st != GST_OK:
             raise GstError(st, "gst_query_batch")
         out = [self._unpack(int(statuses[i]), res[i], bufs[i]) for i in range(n)]
@@ -289,8 +321,10 @@ class Server:
             raise GstError(st, "gst_serve_open")
         self._h = h
 
-    def submit(self, req_id: int, groups, D: int = -1) -> int:
+    def submit(self, req_id: int, groups, D: int = -1, ratio: float = 0.0) -> int:
         g = np.ascontiguousarray(groups, dtype=np.uint32)
+        if ratio:
+            return int(lib().gst_serve_submit_ratio(self._h, int(req_id), _ptr(g), len(g), int(D), float(ratio)))
         return int(lib().gst_serve_submit(self._h, int(req_id), _ptr(g), len(g), int(D)))
 
     def poll(self, max_results: int = 1024, max_edges: int = 0):
@@ -315,6 +349,23 @@ class Server:
             buf = bufs[i] if max_edges else np.zeros(0, dtype=np.uint32)
             out.append((int(ids[i]), Engine._unpack(int(sts[i]), res[i], buf)))
         return out
+
+    def cancel(self, req_id: int) -> int:
+        """Withdraw a request (gst_serve_cancel): GST_OK or GST_NOT_FOUND."""
+        return int(lib().gst_serve_cancel(self._h, int(req_id)))
+
+    def set_max_pending(self, n: int):
+        st = lib().gst_serve_set_max_pending(self._h, int(n))
+        if st != GST_OK:
+            raise GstError(st, "gst_serve_set_max_pending")
+
+    def stats(self) -> dict:
+        """Occupancy and counters (gst_serve_stats)."""
+        info = _ServeInfo()
+        st = lib().gst_serve_stats(self._h, ctypes.byref(info))
+        if st != GST_OK:
+            raise GstError(st, "gst_serve_stats")
+        return {n: int(getattr(info, n)) for n, _ in _ServeInfo._fields_}
 
     def close(self):
         if getattr(self, "_h", None):

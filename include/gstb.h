@@ -53,7 +53,8 @@ typedef enum gst_status {
   GST_INTERNAL = 8,         /* internal consistency check failed */
   GST_BUSY = 9,             /* serving: no free slot right now (submit again) */
   GST_NOT_FOUND = 10,       /* serving: unknown request id */
-  GST_SCRATCH_TOO_SMALL = 11  /* gst_query_noalloc: workspace exceeds the static scratch */
+  GST_SCRATCH_TOO_SMALL = 11, /* gst_query_noalloc: workspace exceeds the static scratch */
+  GST_CANCELLED = 12        /* serving: the request was withdrawn by gst_serve_cancel */
 } gst_status;
 
 typedef struct gst_graph gst_graph;
@@ -73,7 +74,8 @@ enum {
   GST_STAT_SSSP_UPDATES = 9,  /* successful distance lowerings */
   GST_STAT_SSSP_ENQUEUED = 10, /* distance frontier insertions */
   GST_STAT_RETRIES = 11,    /* runs repeated with 4x larger frontier lists after GST_QUEUE_OVERFLOW */
-  GST_NSTATS = 12
+  GST_STAT_LOWER_BOUND = 12,  /* proven lower bound on the optimum (= cost for an exact answer) */
+  GST_NSTATS = 13
 };
 
 typedef struct gst_result {
@@ -91,7 +93,9 @@ typedef struct gst_result {
 /* Replaces toCSR (code/GPUGST/include/graph_v_of_v_idealID/csr_graph.hpp:39-128):
  * copies a symmetric CSR (beg_pos[V+1], csr[arcs], w[arcs]; both directions
  * of every undirected edge present; weights >= 1) to the device.  The library
- * keeps its own device copy with each adjacency list re-sorted by weight. */
+ * keeps its own device copy with each adjacency list re-sorted by weight.
+ * Costs are summed in 32 bits: a graph whose V-1 heaviest arcs weigh 2^30 or
+ * more in total (the bound on any shortest path or tree) is GST_BAD_INPUT. */
 gst_status gst_graph_create(const uint32_t* beg_pos, const uint32_t* csr, const int32_t* w,
                             uint32_t V, uint64_t arcs, gst_graph** out);
 
@@ -111,6 +115,20 @@ uint64_t gst_graph_num_arcs(const gst_graph* g);
  * tree (the reference's GPU path returns the cost only; its extraction is
  * commented out at DPQ.cu:577-606). */
 gst_status gst_query(gst_graph* g, const uint32_t* groups, int k, int D, gst_result* out);
+
+/* Progressive mode (the reference's maximum_return_app_ratio,
+ * code/PrunedDP++/include/CPUNONHOP.h:499,730-755): the query may stop before
+ * the DP has proven optimality, once the best tree recorded costs at most
+ * `ratio` times a proven lower bound on the optimum.  The returned cost is
+ * then at most ratio x the optimum, and stats[GST_STAT_LOWER_BOUND] holds the
+ * bound.  The comparison is exact integer arithmetic (ratio is taken in
+ * steps of 1/1024, rounded down), unlike the reference's integer division
+ * (CPUNONHOP.h:733), which returns up to 2x the optimum at ratio 1.  The tree
+ * is the minimum spanning tree of the recorded derivation's edges, as the
+ * reference post-processes its incumbent.  ratio <= 1 is the exact query.
+ * Hop-bounded queries (D >= 0) are always exact: the reference's hop program
+ * (CPUHOP.h) has no ratio exit either. */
+gst_status gst_query_ratio(gst_graph* g, const uint32_t* groups, int k, int D, double ratio, gst_result* out);
 
 /* Allocation-free variant of gst_query.  It has no counterpart in the
  * reference.  Some callers cannot allocate device memory while they answer a
@@ -132,7 +150,10 @@ gst_status gst_query(gst_graph* g, const uint32_t* groups, int k, int D, gst_res
  *     before any stream capture.
  *   - All calls share the array; each call re-initialises what must start
  *     empty.  Calls that overlapped on the GPU would race on it, so the
- *     library serialises its own calls with a mutex.
+ *     library serialises its own calls with a mutex.  A call also holds the
+ *     graph's lock, so on one graph it waits for (and holds off)
+ *     gst_query, gst_query_batch, gst_tuning_set and gst_autotune, and it
+ *     reads the group index under the lock gst_groups_set takes.
  * Trees are returned with up to 4096 edges (GST_TRUNCATED beyond).  The
  * call switches to the graph's device for its duration and restores the
  * caller's current device before returning. */
@@ -174,6 +195,11 @@ gst_status gst_autotune(gst_graph* g, int n, const uint32_t* groups, const int32
 gst_status gst_query_batch(gst_graph* g, int n, const uint32_t* groups, const int32_t* ks,
                            const int32_t* Ds, gst_result* results, int32_t* statuses,
                            int max_concurrent);
+/* gst_query_batch with a progressive-mode ratio per query (ratios may be
+ * null: every query exact; see gst_query_ratio). */
+gst_status gst_query_batch_ratio(gst_graph* g, int n, const uint32_t* groups, const int32_t* ks,
+                                 const int32_t* Ds, const double* ratios, gst_result* results,
+                                 int32_t* statuses, int max_concurrent);
 
 /* Serving loop (continuous batching).  A background host thread keeps the
  * graph resident, admits submitted queries as device memory frees up, and
@@ -189,14 +215,42 @@ gst_status gst_serve_open(gst_graph* g, uint64_t hbm_budget_bytes, int max_infli
                           gst_server** out);
 /* Never blocks.  Copies the groups.  GST_BUSY if the pending queue is full. */
 gst_status gst_serve_submit(gst_server* s, uint64_t req_id, const uint32_t* groups, int k, int D);
+/* gst_serve_submit in progressive mode (see gst_query_ratio). */
+gst_status gst_serve_submit_ratio(gst_server* s, uint64_t req_id, const uint32_t* groups, int k, int D,
+                                  double ratio);
 /* Returns up to max_results finished requests; *n_out set.  Tree edges are
  * copied into each result's caller buffer (edges/max_edges preset by the
  * caller; pass max_edges 0 to skip trees).  ids[i] and statuses[i] filled. */
 gst_status gst_serve_poll(gst_server* s, uint64_t* ids, int32_t* statuses, gst_result* results,
                           int max_results, int* n_out);
+/* Withdraws a request.  A pending request (not yet on the device) finishes at
+ * once; an admitted one is ended by the device at its next round.  Either way
+ * it is reported by gst_serve_poll with status GST_CANCELLED, unless it
+ * finished first (then it keeps its own result).  GST_NOT_FOUND if no pending
+ * or admitted request has this id.  No reference counterpart. */
+gst_status gst_serve_cancel(gst_server* s, uint64_t req_id);
+/* Largest number of pending (submitted, not yet admitted) requests; a submit
+ * beyond it returns GST_BUSY (load shedding).  Default 2^20. */
+gst_status gst_serve_set_max_pending(gst_server* s, uint64_t max_pending);
+/* Occupancy and counters of a server (the quantities a front-end routes on). */
+typedef struct gst_serve_info {
+  uint64_t pending;            /* submitted, waiting for admission */
+  uint64_t inflight;           /* admitted, on the device */
+  uint64_t finished_unpolled;  /* finished, not yet returned by gst_serve_poll */
+  uint64_t budget_bytes;       /* HBM budget of the admitted workspaces */
+  uint64_t in_use_bytes;       /* workspace bytes of the admitted requests */
+  uint64_t submitted, completed, rejected_busy, cancelled, oom;  /* totals since open */
+} gst_serve_info;
+gst_status gst_serve_stats(gst_server* s, gst_serve_info* out);
 /* Stops the loop after the submitted requests finish and frees everything;
  * results not polled by then are discarded. */
 gst_status gst_serve_close(gst_server* s);
+
+/* Fault injection for tests (no reference counterpart): the next n workspace
+ * allocations of this graph's engines fail as if the device were full.  A
+ * query that cannot be admitted while nothing else runs returns GST_OOM;
+ * with others running it waits for their memory. */
+gst_status gst_debug_fail_allocs(gst_graph* g, int n);
 
 const char* gst_status_string(gst_status st);
 /* The CUDA runtime's description of the last CUDA error any gstb call in this

@@ -25,7 +25,9 @@ sys.path.insert(0, ROOT)
 from gpugst_b200 import formats, gen  # noqa: E402
 
 REF_BIN = os.path.join(ROOT, "oracle", "_ref")
-GSTP = "/root/reference/code/GPUGST/simple_iterative_tests.text"
+# the reference tree: GSTB_REFERENCE_ROOT when set, else its mount point here
+REF_ROOT = os.environ.get("GSTB_REFERENCE_ROOT", "/root/reference")
+GSTP = os.path.join(REF_ROOT, "code", "GPUGST", "simple_iterative_tests.text")
 
 # instance name -> generator spec (regenerated identically by the tests)
 SPECS = {

@@ -164,3 +164,106 @@ def test_cli_matches_oracle(tmp_path, oracle_mod):
         h = O.hop(g, gr, q, 4)
         want.append(h.cost if h.status == 0 else 0)
     assert costs == want
+
+
+def test_graph_create_rejects_costs_beyond_32_bits(L):
+    """Weights whose V-1 heaviest arcs reach 2^30 in total could overflow the
+    32-bit cost sums: such a graph is rejected on the host."""
+    # 3 vertices, path 0-1-2 with weight 2^29 each way: 2 heaviest arcs = 2^30
+    beg = [0, 1, 3, 4]
+    csr = [1, 0, 2, 1]
+    w = [1 << 29] * 4
+    st, _ = _create(L, beg, csr, w)
+    assert st == 2
+    w = [(1 << 29) - 1] * 4  # just below: accepted (no device needed to validate; creation may fail later)
+    st, h = _create(L, beg, csr, w)
+    assert st != 2
+
+
+def _slow_path_instance():
+    """A path of 3000 vertices with weight 100 per edge and the two end
+    vertices as the only query groups: with a distance window of width 1 the
+    query runs for thousands of rounds, long enough to be withdrawn."""
+    V = 3000
+    u = np.arange(V - 1)
+    g = gen.csr_from_edges(V, u, u + 1, np.full(V - 1, 100, dtype=np.int32))
+    ptr = np.array([0, 1, 2, 3], dtype=np.uint64)
+    mem = np.array([0, V - 1, V // 2], dtype=np.uint32)
+    return g, gen.Groups(ptr, mem)
+
+
+def _poll_all(S, n, timeout=60.0):
+    import time
+    got = {}
+    t0 = time.time()
+    while len(got) < n and time.time() - t0 < timeout:
+        for rid, r in S.poll():
+            got[rid] = r
+        time.sleep(0.001)
+    return got
+
+
+@pytest.mark.gpu
+def test_serve_cancel_pending_and_running(gst_lib):
+    """gst_serve_cancel withdraws a pending request at once and an admitted one
+    at its next device round; both come back as GST_CANCELLED.  Load shedding:
+    beyond max_pending a submit returns GST_BUSY.  Unknown ids are NOT_FOUND."""
+    import time
+    eng = gst_lib
+    g, gr = _slow_path_instance()
+    E = eng.Engine.from_instance(g, gr)
+    E.set_tuning(delta_sssp=1, delta_dp=1, cap_pct=100)
+    quick = [np.array([2], dtype=np.uint32)] * 3          # k = 1: cost 0, a few rounds
+    S = eng.Server(E, max_inflight=1)
+    S.set_max_pending(3)
+    assert S.submit(0, [0, 1]) == eng.GST_OK             # slow: occupies the only slot
+    t0 = time.time()
+    while S.stats()["inflight"] < 1 and time.time() - t0 < 10:
+        time.sleep(0.001)
+    for i, q in enumerate(quick):
+        assert S.submit(10 + i, q) == eng.GST_OK          # pending behind it
+    assert S.submit(99, quick[0]) == eng.GST_BUSY          # beyond max_pending
+    assert S.cancel(11) == eng.GST_OK                     # pending: finished at once
+    assert S.cancel(12345) == eng.GST_NOT_FOUND
+    assert S.cancel(0) == eng.GST_OK                      # running: ended on the device
+    got = _poll_all(S, 4)
+    st = S.stats()
+    S.close()
+    E.close()
+    assert got[0].status == eng.GST_CANCELLED, got[0].status
+    assert got[11].status == eng.GST_CANCELLED
+    assert got[10].status == eng.GST_OK and got[10].cost == 0
+    assert got[12].status == eng.GST_OK and got[12].cost == 0
+    assert st["rejected_busy"] == 1 and st["cancelled"] == 2 and st["completed"] == 4
+
+
+@pytest.mark.gpu
+def test_injected_allocation_failure_is_reported_and_recovered(gst_lib):
+    """A workspace allocation that fails while nothing else runs gives GST_OOM
+    for that query only; the next queries are served with the same results
+    (plain path and serving loop)."""
+    eng = gst_lib
+    g, gr, qs = gen.config1()
+    E = eng.Engine.from_instance(g, gr)
+    q = qs[3][0]
+    base = E.query(q)
+    assert base.ok
+    E.fail_allocs(1)
+    r = E.query(q)
+    assert r.status == eng.GST_OOM
+    r = E.query(q)
+    assert r.ok and r.cost == base.cost
+    S = eng.Server(E, max_inflight=4)
+    E.fail_allocs(1)
+    assert S.submit(0, q) == eng.GST_OK
+    got = _poll_all(S, 1)
+    assert got[0].status == eng.GST_OOM
+    for i in range(1, 6):
+        assert S.submit(i, qs[3][i]) == eng.GST_OK
+    got.update(_poll_all(S, 5))
+    st = S.stats()
+    S.close()
+    want = [E.query(qs[3][i]).cost for i in range(1, 6)]
+    E.close()
+    assert [got[i].cost for i in range(1, 6)] == want
+    assert st["oom"] == 1 and st["completed"] == 6

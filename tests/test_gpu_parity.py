@@ -242,3 +242,58 @@ def test_autotune_keeps_results_exact(gst_lib, oracle_mod, c1):
         r = E.query(q)
         assert r.status == eng.GST_OK and r.cost == O.prunedpp(g, gr, q, 0).cost
     E.close()
+
+
+def test_progressive_mode(gst_lib, oracle_mod, c1):
+    """Progressive mode (gst_query_ratio / gst_query_batch_ratio /
+    gst_serve_submit_ratio): the cost is at least the optimum and at most
+    ratio x the optimum (and ratio x the reported lower bound, which is at
+    most the optimum); the tree is valid; ratio <= 1 and hop-bounded queries
+    are exact."""
+    import time
+    eng, O = gst_lib, oracle_mod
+    bad = []
+    insts = [(c1[0], c1[1], list(c1[2][3][:16]))]
+    for g, gr, q in small_cases(8, seed0=900, V=2000, E=12000, n_groups=150, smax=10, kmax=6):
+        insts.append((g, gr, [q]))
+    early = 0
+    for g, gr, queries in insts:
+        E = _engine(eng, g, gr)
+        for q in queries:
+            opt = O.prunedpp(g, gr, q, 0).cost
+            for ratio in (1.0, 1.25, 1.5, 2.0, 4.0):
+                r = E.query(q, ratio=ratio)
+                lb = r.stats["lower_bound"]
+                if r.status != eng.GST_OK or not (opt <= r.cost <= int(ratio * opt)) or lb > opt:
+                    bad.append((q.tolist(), ratio, opt, r.status, r.cost, lb))
+                    continue
+                if r.cost > ratio * lb or (ratio <= 1.0 and r.cost != opt):
+                    bad.append((q.tolist(), ratio, "bound", opt, r.cost, lb))
+                if O.validate(g, gr, q, -1, r.cost, r.root, r.edges):
+                    bad.append((q.tolist(), ratio, "invalid tree"))
+                early += lb < opt
+            # hop-bounded queries ignore the ratio
+            h = E.query(q, D=3, ratio=2.0)
+            want = O.hop(g, gr, q, 3)
+            if (want.status == 0) != (h.status == eng.GST_OK) or (want.status == 0 and h.cost != want.cost):
+                bad.append((q.tolist(), "hop", want.cost, h.status, h.cost))
+        # batch and serving entry points agree with the bound
+        res = E.query_batch(queries, ratios=[1.5] * len(queries))
+        S = eng.Server(E, max_inflight=8)
+        for i, q in enumerate(queries):
+            S.submit(i, q, ratio=1.5)
+        got = {}
+        t0 = time.time()
+        while len(got) < len(queries) and time.time() - t0 < 60:
+            for rid, rr in S.poll(max_edges=4096):
+                got[rid] = rr
+            time.sleep(0.001)
+        S.close()
+        for i, q in enumerate(queries):
+            opt = O.prunedpp(g, gr, q, 0).cost
+            for tag, rr in (("batch", res[i]), ("serve", got.get(i))):
+                if rr is None or rr.status != eng.GST_OK or not (opt <= rr.cost <= int(1.5 * opt)):
+                    bad.append((tag, q.tolist(), opt, None if rr is None else (rr.status, rr.cost)))
+        E.close()
+    assert not bad, bad[:10]
+    assert early > 0, "no query stopped early: the progressive exit was never exercised"

@@ -55,3 +55,46 @@ def test_two_gloo_ranks():
     for r in res:
         assert r[3] == [11.0, 5.0]  # max over ranks
         assert r[4] == [90.0]
+
+
+def _leaver(rank, world, port, out):
+    """Two gloo ranks; each step ends with the timing collective (max over
+    ranks).  Rank 1 takes two steps and exits between steps; rank 0 must learn
+    it from the heartbeat at step 2, before it enters that step's collective."""
+    import datetime
+    import torch.distributed as dist
+    store = dist.TCPStore("127.0.0.1", port, world, rank == 0, timeout=datetime.timedelta(seconds=30))
+    dist.init_process_group("gloo", store=store, rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=20))
+    hb = replicas.StepHeartbeat(store, rank, world, timeout_s=3.0)
+    done = []
+    try:
+        for step in range(4):
+            if rank == 1 and step == 2:
+                out.put((rank, "left", done))
+                return  # leaves between steps, nothing in flight
+            hb.step(step)
+            t = replicas.max_over_ranks([float(step + rank)])
+            assert t == [float(step + 1)]
+            done.append(step)
+        out.put((rank, "finished", done))
+    except replicas.RankLost as e:
+        out.put((rank, f"lost {e.rank} at {e.step}", done))
+        # the survivor keeps the store alive until the peer's process is gone
+        import time
+        time.sleep(0.5)
+
+
+def test_rank_that_leaves_is_detected():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_leaver, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = dict((r, (msg, done)) for r, msg, done in (q.get(timeout=120) for _ in ps))
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res[1] == ("left", [0, 1])
+    assert res[0] == ("lost 1 at 2", [0, 1])
