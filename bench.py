@@ -1,17 +1,25 @@
 #!/usr/bin/env python
-"""Benchmark: exact-optimal group Steiner tree queries/s (+ p50/p99 latency),
-batched engine vs the plain one-query-at-a-time GPU path.
+"""Benchmark: exact-optimal group Steiner tree queries/s with p50/p99 latency,
+batched engine and continuous-batching serving loop vs the plain
+one-query-at-a-time GPU path.
 
-Workload (default "c2"): Chung-Lu power-law graph, V=170,000, E=6.8M undirected
-(13.6M arcs), exponent 2.3, int32 weights uniform in [1,100]; 200,000 groups
-with Zipf(1.5) sizes in [1,200]; 300 queries each at k = 3, 4, 5 (seeded
-synthetic stand-in for the reference's datasets).  One step = one batch of
---batch queries through gst_query_batch (host buffers in, costs and trees out).
+Workloads (seeded synthetic stand-ins for the reference's datasets):
+  c4 (default, the batched configuration): Chung-Lu power-law graph,
+     V=3,000,000, E=117M undirected (234M arcs), exponent 2.1, int32 weights
+     uniform in [1,100]; 1,000,000 groups with Zipf(1.3) sizes in [1,500]; a
+     set of 1,024 queries with k uniform in {3,4,5,6}, half of them with a hop
+     bound D uniform in {2,3,4}.  One step = one gst_query_batch call over
+     --batch queries taken in order from that set (cycling), host buffers in,
+     costs and trees out.  The open-loop serving configuration (c5: the same
+     graph, Poisson arrivals) is measured in the same run.
+  c2: Chung-Lu V=170,000, E=6.8M (13.6M arcs), exponent 2.3; 200,000 groups
+     with Zipf(1.5) sizes in [1,200]; 300 queries each at k = 3, 4, 5.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+                  [--workload c4|c2]
 
-N > 1 runs one replica per GPU (queries are independent: each rank takes its
-own share of the query stream; no collective on the data path).
+N > 1 runs one replica per GPU (queries are independent: each rank answers
+its own share of the query stream; no collective on the data path).
 """
 from __future__ import annotations
 
@@ -33,7 +41,12 @@ CACHE = os.environ.get("GSTB_CACHE", "/tmp/gstb_cache")
 METRIC = "exact-optimal queries/sec + p50/p99 latency: batched serve vs plain per-query GPU"
 
 
+# ---------------------------------------------------------------------------
+# Workloads
+# ---------------------------------------------------------------------------
+
 def load_workload(name: str):
+    """(graph, groups, queries, Ds): the workload's query list in bench order."""
     from gpugst_b200 import gen
     os.makedirs(CACHE, exist_ok=True)
     path = os.path.join(CACHE, f"{name}.npz")
@@ -41,29 +54,39 @@ def load_workload(name: str):
         z = np.load(path)
         g = gen.Graph(len(z["beg"]) - 1, z["beg"], z["csr"], z["w"])
         gr = gen.Groups(z["gp"], z["gv"])
-        qs = {int(k[1:]): z[k] for k in z.files if k.startswith("q")}
-        return g, gr, qs
-    if name == "c2":
-        g, gr, qs = gen.config2()
-    elif name == "c1":
-        g, gr, qs = gen.config1()
+        qs = [row[:k].astype(np.uint32) for row, k in zip(z["qs"], z["ks"])]
+        return g, gr, qs, [int(d) for d in z["Ds"]]
+    if name == "c4":
+        g, gr, qs, Ds = gen.config4()
+    elif name in ("c1", "c2"):
+        g, gr, per_k = gen.config1() if name == "c1" else gen.config2()
+        ks = sorted(per_k)
+        n = min(len(per_k[k]) for k in ks)
+        qs = [per_k[k][i] for i in range(n) for k in ks]  # k = 3, 4, 5, 3, 4, 5, ...
+        Ds = [-1] * len(qs)
     else:
         raise SystemExit(f"unknown workload {name}")
-    np.savez(path, beg=g.beg_pos, csr=g.csr, w=g.weight, gp=gr.ptr, gv=gr.members,
-             **{f"q{k}": v for k, v in qs.items()})
-    return g, gr, qs
+    rows = np.zeros((len(qs), 8), dtype=np.uint32)
+    for i, q in enumerate(qs):
+        rows[i, :len(q)] = q
+    np.savez(path, beg=g.beg_pos, csr=g.csr, w=g.weight, gp=gr.ptr, gv=gr.members, qs=rows,
+             ks=np.array([len(q) for q in qs]), Ds=np.array(Ds))
+    return g, gr, qs, Ds
 
 
-def query_pool(qs):
-    """Interleave the per-k query sets: k=3,4,5,3,4,5,..."""
-    ks = sorted(qs)
-    n = min(len(qs[k]) for k in ks)
-    pool = []
-    for i in range(n):
-        for k in ks:
-            pool.append(qs[k][i])
-    return pool
+def workload_desc(name):
+    if name == "c4":
+        return ("chung-lu V=3000000 E=117M gamma=2.1 w~U[1,100]; 1000000 zipf(1.3) groups in [1,500]; "
+                "1024 queries k~U{3..6}, half with D~U{2,3,4}")
+    if name == "c2":
+        return ("chung-lu V=170000 E=6.8M gamma=2.3 w~U[1,100]; 200000 zipf(1.5) groups in [1,200]; "
+                "queries k=3,4,5 interleaved (300 each)")
+    return name
 
+
+# ---------------------------------------------------------------------------
+# Measurement helpers
+# ---------------------------------------------------------------------------
 
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
@@ -131,6 +154,10 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
+def pct(xs, p):
+    return float(np.percentile(np.array(xs), p)) if len(xs) else None
+
+
 # Algorithmic bytes of a round, from the device counters (the useful bytes
 # each unit of work must move).  The two round kernels share the work types
 # (k_light: distance items and DP states; k_heavy: the arc chunks k_light
@@ -149,10 +176,9 @@ def distance_work_bytes(st):
     return 48 * st["sssp_items"] + 40 * st["sssp_arcs"] + 4 * st["sssp_updates"] + 8 * st["sssp_enqueued"]
 
 
-def dp_work_bytes(st, V, ks):
-    lb_rows = sum(V * (32 + 2 * (1 << k)) for k in ks)
+def dp_work_bytes(st, lb_rows_bytes):
     return (66 * st["expanded"] + 18 * st["arcs"] + 10 * st["merges"] + 8 * st["updates"]
-            + 8 * st["enqueued"] + lb_rows)
+            + 8 * st["enqueued"] + lb_rows_bytes)
 
 
 def traffic_per_byte():
@@ -166,128 +192,202 @@ def traffic_per_byte():
     return d.get("dram_bytes_per_algorithmic_byte")
 
 
-def cpu_baseline_port(g, gr, pool, n_per_k=3):
-    """The oracle restatement of PrunedDP++ (exact mode) on one core."""
+# ---------------------------------------------------------------------------
+# CPU baseline (oracle restatement) -- run before CUDA is initialised so the
+# worker processes can be forked with the graph shared copy-on-write
+# ---------------------------------------------------------------------------
+
+_CPU = {}
+
+
+def _cpu_one(i):
+    from oracle import oracle
+    q, D = _CPU["qs"][i], _CPU["Ds"][i]
+    t0 = time.perf_counter()
+    r = oracle.prunedpp(_CPU["g"], _CPU["gr"], q, 0) if D < 0 else oracle.hop(_CPU["g"], _CPU["gr"], q, D)
+    return i, r.status, r.cost, time.perf_counter() - t0
+
+
+def cpu_baseline_port(g, gr, qs, Ds, workload):
+    """The PrunedDP++ restatement (exact mode; HOP_cpu restatement for
+    hop-bounded queries) on a bounded sample of the workload: one query per
+    host core, all cores in parallel.  Returns (cpu_baseline dict, {query
+    index: (status, cost)}) -- the costs are the bench's parity check."""
+    import multiprocessing as mp
     from oracle import oracle
     oracle.build()
-    sample = []
-    seen = {}
-    for q in pool:
-        k = len(q)
-        if seen.get(k, 0) < n_per_k:
-            sample.append(q)
-            seen[k] = seen.get(k, 0) + 1
+    cores = max(1, min(os.cpu_count() or 1, 32))
+    if workload == "c4":
+        # unbounded k = 3 queries: the restatement takes about 30 s each on
+        # this graph (k = 6 takes minutes)
+        sample = [i for i in range(len(qs)) if Ds[i] < 0 and len(qs[i]) == 3][:cores]
+    else:
+        sample = list(range(min(len(qs), 3 * cores)))
+    _CPU.update(g=g, gr=gr, qs=qs, Ds=Ds)
     t0 = time.perf_counter()
-    for q in sample:
-        oracle.prunedpp(g, gr, q, 0)
-    dt = time.perf_counter() - t0
-    return {"value": len(sample) / dt, "unit": "queries/s", "cores": 1, "kind": "port",
-            "sample": f"{len(sample)} queries ({n_per_k} each of k={sorted(seen)}) of the same workload, "
-                      f"PrunedDP++ restatement (exact mode), {dt:.1f} s"}
+    with mp.get_context("fork").Pool(cores) as pool:
+        out = pool.map(_cpu_one, sample, chunksize=1)
+    wall = time.perf_counter() - t0
+    costs = {i: (st, c) for i, st, c, _ in out}
+    busy = sum(x[3] for x in out)
+    return ({"value": len(sample) / wall, "unit": "queries/s", "cores": cores, "kind": "port",
+             "sample": f"{len(sample)} queries of the workload (k in {sorted(set(len(qs[i]) for i in sample))}, "
+                       f"{sum(Ds[i] >= 0 for i in sample)} hop-bounded), PrunedDP++ / HOP_cpu restatement in exact "
+                       f"mode, one query per process on {cores} cores; {wall:.1f} s wall, {busy:.1f} s busy"},
+            costs)
 
 
-def ref_dataset(name, g, gr, pool):
-    """Write the workload in the reference's file formats (cached)."""
+# ---------------------------------------------------------------------------
+# Reference arm: the reference's own PrunedDP++ program (oracle/_ref)
+# ---------------------------------------------------------------------------
+
+def ref_dataset(name, g, gr, qs, Ds):
+    """The workload's unbounded queries in the reference's file formats (cached):
+    <name>.in, <name>.g and <name><k>.csv per k."""
     from gpugst_b200 import formats
     d = os.path.join(CACHE, f"ref_{name}")
     if not os.path.exists(os.path.join(d, "done")):
-        qs = {}
-        for q in pool:
-            qs.setdefault(len(q), []).append(q)
-        formats.write_dataset(d, name, g, gr, {k: np.array(v) for k, v in qs.items()})
+        byk = {}
+        for q, D in zip(qs, Ds):
+            if D < 0:
+                byk.setdefault(len(q), []).append(q)
+        formats.write_dataset(d, name, g, gr, {k: np.array(v) for k, v in byk.items()})
         open(os.path.join(d, "done"), "w").close()
     return d + "/"
 
 
-def run_reference(args, g, gr, pool, rank, world):
-    """--impl reference: the reference's own PrunedDP++ CPU program (oracle/_ref,
-    compiled from the reference sources) on all usable host cores, one query per
-    core per step; falls back to the oracle restatement when it is absent."""
+def run_reference(args, g, gr, qs, Ds, rank, world):
+    """--impl reference: the reference's own PrunedDP++ CPU program
+    (oracle/_ref/prunedpp_ref, compiled from the reference sources) on the
+    workload's unbounded queries, one long-lived process per host core, each
+    answering its own queries one after another (the reference's per-query
+    loop, exp_CPU_nonHop.h:97-138).  A step is one query per process; the
+    line's throughput is all timed queries / the busiest process's summed
+    query time."""
     if rank != 0:
         return
     ref_bin = os.path.join(ROOT, "oracle", "_ref", "prunedpp_ref")
     nproc = os.cpu_count() or 1
     try:
         import psutil
-        mem_workers = int(psutil.virtual_memory().available / (3 << 30))
+        per_proc = (12 << 30) if args.workload == "c4" else (3 << 30)
+        mem_workers = int(psutil.virtual_memory().available / per_proc)
     except Exception:
         mem_workers = nproc
     workers = max(1, min(nproc, 32, mem_workers))
     steps = args.steps + args.warmup
-    if os.path.exists(ref_bin):
-        kind = "reference"
-        d = ref_dataset(args.workload, g, gr, pool)
-        # worker w runs the queries w, w + workers, ... of the k-interleaved pool, grouped by k file
-        byk = {}
-        for q in pool:
+    if not os.path.exists(ref_bin):
+        raise SystemExit("oracle/_ref/prunedpp_ref missing: build it with make -C oracle ref")
+    d = ref_dataset(args.workload, g, gr, qs, Ds)
+    byk = {}
+    for q, D in zip(qs, Ds):
+        if D < 0:
             byk.setdefault(len(q), []).append(q)
-        procs = []
-        assign = []  # (worker, k, index)
-        for w in range(workers):
-            ks = sorted(byk)
-            k = ks[w % len(ks)]
-            base = (w // len(ks)) * steps
-            assign.append((k, base))
-            procs.append(subprocess.Popen([ref_bin, d, args.workload, str(k), str(base), str(base + steps - 1), "0"],
-                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
-        per = []
-        for p in procs:
-            out, _ = p.communicate()
-            secs = [float(line.split()[4]) for line in out.splitlines() if line.startswith("RESULT ")]
-            per.append(secs)
-        step_times = []
-        for s in range(args.warmup, steps):
-            step_times.append(max(x[s] for x in per if len(x) > s))
-        nq = workers * args.steps
-        total = sum(step_times)
-        sample = (f"{args.steps} steps x {workers} concurrent processes (one query each; k cycles 3,4,5); "
-                  f"step time = slowest process's query time; graph load excluded")
-    else:
-        kind = "port"
-        from oracle import oracle
-        oracle.build()
-        import multiprocessing as mp
-        ctx = mp.get_context("spawn")
-        total = 0.0
-        nq = 0
-        with ctx.Pool(workers, initializer=_ref_init, initargs=(args.workload,)) as pool_ex:
-            for s in range(steps):
-                batch = [pool[(s * workers + i) % len(pool)] for i in range(workers)]
-                t0 = time.perf_counter()
-                pool_ex.map(_ref_one, batch)
-                dt = time.perf_counter() - t0
-                if s >= args.warmup:
-                    total += dt
-                    nq += len(batch)
-        sample = f"{args.steps} steps x {workers} queries in parallel processes (oracle restatement)"
-    value = nq / total
+    ks = sorted(byk)
+    procs = []
+    for w in range(workers):
+        k = ks[w % len(ks)]
+        base = ((w // len(ks)) * steps) % max(1, len(byk[k]) - steps)
+        procs.append(subprocess.Popen([ref_bin, d, args.workload, str(k), str(base), str(base + steps - 1), "0"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
+    per = []
+    for p in procs:
+        out, _ = p.communicate()
+        per.append([float(line.split()[4]) for line in out.splitlines() if line.startswith("RESULT ")])
+    timed = [x[args.warmup:steps] for x in per]
+    nq = sum(len(x) for x in timed)
+    busy_max = max(sum(x) for x in timed)
+    value = nq / busy_max
     line = {"metric": METRIC, "value": value, "unit": "queries/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * busy_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-            "data": "synthetic", "config": {"workload": workload_desc(args.workload)},
-            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": workers, "kind": kind, "sample": sample},
+            "data": "synthetic", "config": {"workload": workload_desc(args.workload),
+                                            "queries": "the workload's unbounded queries (PrunedDP++ has no hop bound)"},
+            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": workers, "kind": "reference",
+                             "sample": f"{workers} processes x {args.steps} timed queries each (k cycling "
+                                       f"{ks}) after {args.warmup} warm-up queries; throughput = all timed "
+                                       f"queries / the busiest process's summed query time; graph load excluded"},
             "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-_REF_STATE = {}
+# ---------------------------------------------------------------------------
+# GPU legs
+# ---------------------------------------------------------------------------
+
+def closed_loop(eng, E, reqs, inflight, ratio=0.0):
+    """Serve reqs [(q, D)] keeping `inflight` on the device: (q/s, latencies ms, statuses)."""
+    S = eng.Server(E, max_inflight=inflight)
+    lat, sts = [], []
+    n = len(reqs)
+    t0 = time.perf_counter()
+    for i in range(min(inflight, n)):
+        S.submit(i, reqs[i][0], reqs[i][1], ratio=ratio)
+    nxt = min(inflight, n)
+    done = 0
+    while done < n:
+        got = S.poll()
+        if not got:
+            time.sleep(0.0002)
+            continue
+        for rid, r in got:
+            lat.append(r.latency_ms)
+            sts.append(r.status)
+            done += 1
+            if nxt < n:
+                S.submit(nxt, reqs[nxt][0], reqs[nxt][1], ratio=ratio)
+                nxt += 1
+    wall = time.perf_counter() - t0
+    S.close()
+    return n / wall, lat, sts
 
 
-def _ref_init(name):
-    g, gr, _ = load_workload(name)
-    _REF_STATE["g"], _REF_STATE["gr"] = g, gr
-
-
-def _ref_one(q):
-    from oracle import oracle
-    return oracle.prunedpp(_REF_STATE["g"], _REF_STATE["gr"], q, 0).cost
-
-
-def workload_desc(name):
-    if name == "c2":
-        return ("chung-lu V=170000 E=6.8M gamma=2.3 w~U[1,100]; 200000 zipf(1.5) groups in [1,200]; "
-                "queries k=3,4,5 interleaved (300 each)")
-    return name
+def open_loop(eng, E, reqs, rate, seconds, seed, max_pending, drain_s):
+    """Poisson arrivals at `rate` q/s for `seconds`: every arrival is submitted
+    at its time (GST_BUSY beyond max_pending pending requests: shed).  After
+    the arrival window the server gets drain_s more seconds; what is still
+    unfinished then is withdrawn with gst_serve_cancel."""
+    from gpugst_b200 import gen
+    arr = gen.poisson_arrivals(rate, seconds, seed)
+    S = eng.Server(E)
+    S.set_max_pending(max_pending)
+    shed, results = 0, {}
+    t0 = time.perf_counter()
+    i = 0
+    while i < len(arr) or time.perf_counter() - t0 < seconds:
+        now = time.perf_counter() - t0
+        while i < len(arr) and arr[i] <= now:
+            q, D = reqs[i % len(reqs)]
+            if S.submit(i, q, D) == eng.GST_BUSY:
+                shed += 1
+            i += 1
+        for rid, r in S.poll():
+            results[rid] = r
+        time.sleep(0.0005)
+    t_end = time.perf_counter() - t0
+    submitted = len(arr) - shed
+    while len(results) < submitted and time.perf_counter() - t0 < t_end + drain_s:
+        for rid, r in S.poll():
+            results[rid] = r
+        time.sleep(0.001)
+    t_drain = time.perf_counter() - t0
+    for rid in range(len(arr)):
+        if rid not in results:
+            S.cancel(rid)
+    t1 = time.perf_counter()
+    while len(results) < submitted and time.perf_counter() - t1 < 60:
+        for rid, r in S.poll():
+            results[rid] = r
+        time.sleep(0.001)
+    st = S.stats()
+    S.close()
+    ok = [r for r in results.values() if r.status in (eng.GST_OK, eng.GST_NO_SOLUTION)]
+    lat = [r.latency_ms for r in ok]
+    return {"offered_qps": rate, "seconds": seconds, "arrivals": int(len(arr)), "shed_busy": shed,
+            "completed": len(ok), "completed_qps": len(ok) / t_drain,
+            "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+            "cancelled_unfinished": sum(r.status == eng.GST_CANCELLED for r in results.values()),
+            "oom": st["oom"], "max_pending": max_pending, "drain_s": drain_s}
 
 
 def main():
@@ -296,24 +396,35 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2")
-    ap.add_argument("--batch", type=int, default=90, help="queries per step")
-    ap.add_argument("--plain", type=int, default=30, help="queries timed on the plain per-query path")
+    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c1"])
+    ap.add_argument("--batch", type=int, default=0, help="queries per step (default: 128 on c4, 90 on c2)")
+    ap.add_argument("--plain", type=int, default=300, help="queries on the plain per-query path")
+    ap.add_argument("--sweep", default="1,2,4,8,16,32", help="closed-loop serving concurrencies")
+    ap.add_argument("--sweep-queries", type=int, default=0, help="queries per sweep point (default 64 on c4)")
+    ap.add_argument("--c5-rates", default="50,200,1000", help="open-loop Poisson rates (c4 only)")
+    ap.add_argument("--c5-seconds", type=float, default=10.0, help="arrival window per rate")
+    ap.add_argument("--c5-max-pending", type=int, default=256)
+    ap.add_argument("--c5-drain", type=float, default=5.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--serve", type=int, default=360, help="queries through the serving loop")
-    ap.add_argument("--inflight", type=int, default=32, help="serving loop concurrency")
     args = ap.parse_args()
+    big = args.workload == "c4"
+    B = args.batch or (128 if big else 90)
+    n_sweep = args.sweep_queries or (64 if big else 256)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
-    g, gr, qs = load_workload(args.workload)
-    pool = query_pool(qs)
+    g, gr, qs, Ds = load_workload(args.workload)
+    nq_set = len(qs)
 
     if args.impl == "reference":
-        run_reference(args, g, gr, pool, rank, world)
+        run_reference(args, g, gr, qs, Ds, rank, world)
         return
+
+    cpu, cpu_costs = None, {}
+    if rank == 0 and not args.no_cpu:
+        cpu, cpu_costs = cpu_baseline_port(g, gr, qs, Ds, args.workload)
 
     import torch
     torch.cuda.set_device(local)
@@ -327,16 +438,16 @@ def main():
     build.build()
     E = engine.Engine.from_instance(g, gr)
 
-    B = args.batch
-    # this rank's share of the query stream
     def batch_for(step):
+        # this rank's share of the query stream: the set in order, cycling
         base = (rank * (args.steps + args.warmup) + step) * B
-        return [pool[(base + i) % len(pool)] for i in range(B)]
+        idx = [(base + i) % nq_set for i in range(B)]
+        return [qs[i] for i in idx], [Ds[i] for i in idx]
 
     l2_flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     for s in range(args.warmup):
-        E.query_batch(batch_for(s))
+        E.query_batch(*batch_for(s))
     torch.cuda.synchronize()
 
     h2d = d2h = 0
@@ -351,9 +462,9 @@ def main():
     for s in range(args.steps):
         l2_flush.fill_(s & 0xFF)  # write > L2 between steps
         torch.cuda.synchronize()
-        qb = batch_for(args.warmup + s)
+        qb, Db = batch_for(args.warmup + s)
         t0 = time.perf_counter()
-        res = E.query_batch(qb)
+        res = E.query_batch(qb, Db)
         wall_ms.append(1e3 * (time.perf_counter() - t0))
         dev_ms.append(res[0].device_ms)
         lat.extend(r.latency_ms for r in res)
@@ -366,23 +477,38 @@ def main():
     launches = E.kernel_launches() - launches0
     if dist:
         dist.barrier()
-
-    tot_dev = sum(dev_ms)
-    tot_wall = sum(wall_ms)
-    tot_dev, tot_wall = replicas.max_over_ranks([tot_dev, tot_wall], device="cuda")
+    tot_dev, tot_wall = replicas.max_over_ranks([sum(dev_ms), sum(wall_ms)], device="cuda")
     nq_all = B * args.steps * world
     value = nq_all / (tot_dev / 1e3)
     e2e_value = nq_all / (tot_wall / 1e3)
 
+    # parity: the oracle's costs on the cpu sample against the GPU's (batched and plain)
+    parity = None
+    if rank == 0 and cpu_costs:
+        idx = sorted(cpu_costs)
+        res_b = E.query_batch([qs[i] for i in idx], [Ds[i] for i in idx])
+        mism = []
+        for i, r in zip(idx, res_b):
+            st, c = cpu_costs[i]
+            rp = E.query(qs[i], D=Ds[i])
+            for rr in (r, rp):
+                good = (rr.status == engine.GST_OK and st == 0 and rr.cost == c) or \
+                       (rr.status == engine.GST_NO_SOLUTION and st == 1)
+                if not good:
+                    mism.append([i, c, rr.status, rr.cost])
+        parity = {"checked": 2 * len(idx), "mismatches": len(mism), "against": "oracle restatement (exact) on the "
+                  "cpu_baseline sample, batched and plain paths", "first": mism[:3]}
+
     # profiled pass (not timed): round-kernel device time and counters for the roofline
     E.profile(True)
     E.profile_reset()
-    prof_batch = batch_for(args.warmup)
-    E.query_batch(prof_batch)
+    pq, pD = batch_for(args.warmup)
+    E.query_batch(pq, pD)
     light_ms, heavy_ms, prof_rounds, st = E.profile_read()
     E.profile(False)
     dist_bytes = distance_work_bytes(st)
-    dp_bytes = dp_work_bytes(st, g.V, [len(q) for q in prof_batch])
+    lb_rows = sum(g.V * (32 + 2 * (1 << len(q))) for q in pq)
+    dp_bytes = dp_work_bytes(st, lb_rows)
     peak, peak_kind = measured_peak_hbm()
     round_ms = light_ms + heavy_ms
     round_bytes = dist_bytes + dp_bytes
@@ -390,49 +516,35 @@ def main():
     tpb = traffic_per_byte()
     per_round_alg = round_bytes / max(prof_rounds, 1)
 
-    # continuous-batching serving loop (closed loop, `--inflight` requests on the device)
-    n_serve = args.serve
-    S = engine.Server(E, max_inflight=args.inflight) if n_serve > 0 else None
-    serve_q = [pool[(rank * 104729 + 7 * i) % len(pool)] for i in range(n_serve)]
-    lat_serve = []
-    t0 = time.perf_counter()
-    nxt = 0
-    for nxt in range(min(args.inflight, n_serve)):
-        S.submit(nxt, serve_q[nxt])
-    nxt = min(args.inflight, n_serve)
-    done = 0
-    while done < n_serve:
-        got = S.poll()
-        if not got:
-            time.sleep(0.0002)
-            continue
-        for rid, r in got:
-            lat_serve.append(r.latency_ms)
-            done += 1
-            if nxt < n_serve:
-                S.submit(nxt, serve_q[nxt])
-                nxt += 1
-    serve_wall = time.perf_counter() - t0
-    if S is not None:
-        S.close()
-    serve_qps = n_serve / serve_wall if n_serve > 0 else None
-
-    # plain per-query path (one query per call, gst_query), same workload
+    # plain per-query path (one query per call, gst_query), same query set
     plain_lat, plain_dev = [], []
     for i in range(args.plain):
-        q = pool[(rank * 7919 + i * 13) % len(pool)]
+        j = (rank * 7919 + i) % nq_set
         t0 = time.perf_counter()
-        r = E.query(q)
+        r = E.query(qs[j], D=Ds[j])
         plain_lat.append(1e3 * (time.perf_counter() - t0))
         plain_dev.append(r.device_ms)
     plain_qps = len(plain_lat) / (sum(plain_lat) / 1e3) if plain_lat else None
+    plain_dev_qps = len(plain_dev) / (sum(plain_dev) / 1e3) if plain_dev else None
 
-    def pct(xs, p):
-        return float(np.percentile(np.array(xs), p)) if xs else None
+    # closed-loop serving at several concurrencies (the latency / throughput trade-off)
+    sweep = []
+    reqs = [(qs[(rank * 104729 + 7 * i) % nq_set], Ds[(rank * 104729 + 7 * i) % nq_set]) for i in range(n_sweep)]
+    for inflight in [int(x) for x in args.sweep.split(",") if x]:
+        qps, lats, sts = closed_loop(engine, E, reqs, inflight)
+        sweep.append({"inflight": inflight, "qps": qps, "p50_ms": pct(lats, 50), "p99_ms": pct(lats, 99),
+                      "vs_plain": qps / plain_qps if plain_qps else None, "queries": len(reqs)})
 
-    out = None
+    # open-loop Poisson serving on the same resident graph (the c5 configuration)
+    c5 = []
+    if big and args.c5_rates:
+        c5reqs = [(qs[i], Ds[i]) for i in range(nq_set)]
+        for rate in [float(x) for x in args.c5_rates.split(",") if x]:
+            c5.append(open_loop(engine, E, c5reqs, rate, args.c5_seconds, seed=5000 + int(rate),
+                                max_pending=args.c5_max_pending, drain_s=args.c5_drain))
+
     if rank == 0:
-        cpu = None if args.no_cpu else cpu_baseline_port(g, gr, pool)
+        best_pt = max(sweep, key=lambda x: x["qps"]) if sweep else None
         out = {
             "metric": METRIC,
             "value": value,
@@ -447,18 +559,22 @@ def main():
             "dtype": "int32",
             "data": "synthetic",
             "config": {"workload": workload_desc(args.workload), "batch_queries_per_step": B,
+                       "queries": f"the {nq_set}-query set in order, cycling",
                        "parallelism": f"replicas x{world}", "l2": "256 MB buffer written between steps",
                        "queries_ok": n_ok},
             "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
+            "parity": parity,
             "latency_ms": {"batched_p50": pct(lat, 50), "batched_p99": pct(lat, 99),
                            "plain_p50": pct(plain_lat, 50), "plain_p99": pct(plain_lat, 99)},
             "plain_per_query": {"value": plain_qps, "unit": "queries/s", "queries": len(plain_lat),
-                                "device_ms_p50": pct(plain_dev, 50)},
-            "batched_vs_plain": value / plain_qps if plain_qps else None,
-            "serve_vs_plain": serve_qps / plain_qps if (plain_qps and serve_qps) else None,
-            "serve": {"value": serve_qps, "unit": "queries/s", "inflight": args.inflight, "queries": n_serve,
-                      "p50_ms": pct(lat_serve, 50), "p99_ms": pct(lat_serve, 99)},
+                                "device_value": plain_dev_qps, "device_ms_p50": pct(plain_dev, 50)},
+            # like units: device throughput over device throughput, host wall over host wall
+            "batched_vs_plain": {"device": value / plain_dev_qps if plain_dev_qps else None,
+                                 "e2e": e2e_value / plain_qps if plain_qps else None},
+            "serve_sweep": sweep,
+            "serve_vs_plain_best": best_pt["vs_plain"] if best_pt else None,
+            "open_loop": c5,
             "roofline": {"bound": "hbm", "kernel": "round (k_light + k_heavy)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": (per_round_alg * tpb) if tpb else None,

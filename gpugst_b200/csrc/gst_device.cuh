@@ -68,6 +68,9 @@ struct RoundDesc {
   uint32_t sssp_w;        // distance items per warp task this round (set by k_control)
   uint32_t light_warps;   // warps of one k_light launch (set by the host)
   uint32_t nslots;        // 1 + the highest slot in use this round (set by k_control)
+  // work stealing: a warp that finished its first task takes the next one
+  // from these counters (zeroed by k_control every round)
+  uint32_t next_light, next_heavy;
 };
 constexpr uint32_t HUB_CHUNK = 256;     // arcs per chunk (one warp)
 constexpr uint32_t LB_CHUNK = 1u << 22; // bound-table rows (vertices) per query per round

@@ -35,7 +35,7 @@
 namespace gstb {
 __global__ void k_control(QDev*, QCtl*, int, RoundDesc*, uint32_t*);
 __global__ void k_light(const QDev*, RoundDesc*, const uint32_t*, int, GraphDev);
-__global__ void k_heavy(const QDev*, const RoundDesc*, const uint32_t*, int, GraphDev);
+__global__ void k_heavy(const QDev*, RoundDesc*, const uint32_t*, int, GraphDev);
 }  // namespace gstb
 
 using namespace gstb;

@@ -28,6 +28,11 @@
 //              which its GPU path leaves commented out)
 #include "gst_device.cuh"
 
+// Round kernels take their tasks by work stealing (1) or by static striding (0).
+#ifndef GSTB_STEAL
+#define GSTB_STEAL 1
+#endif
+
 namespace gstb {
 
 __device__ __forceinline__ uint32_t warp_sum(uint32_t x) {
@@ -561,6 +566,16 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
     ws_add(ws, q.ctl, ST_ENQ, se);
     ws_add(ws, q.ctl, ST_MERGES, sm);
   }
+}
+
+// Next task of a warp.  Each warp's first task is its own index; after that
+// the warps take tasks from a shared counter (work stealing), so a warp that
+// met cheap tasks keeps taking new ones while one with a long task (a hub
+// vertex, a state with many merge partners) is still busy.
+__device__ __forceinline__ uint32_t next_task(uint32_t* counter, uint32_t nwarps, uint32_t lane) {
+  uint32_t t = 0;
+  if (lane == 0) t = nwarps + atomicAdd(counter, 1u);
+  return __shfl_sync(0xFFFFFFFFu, t, 0);
 }
 
 // Slot owning flat item `it` of task type t: largest s with pre[s] <= it.
@@ -1449,6 +1464,8 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
     rd->n_live = live_cnt;
     rd->nslots = used_hi;  // slots the round kernels search (all later ones are free)
     rd->n_big = 0;
+    rd->next_light = 0;
+    rd->next_heavy = 0;
     // hub chunking pays off only when the round is too small to fill the GPU
     rd->hub_on =
         (rd->big != nullptr && rd->items[T_SSSP] + rd->items[T_DP] + rd->items[T_HOP] < rd->hub_max_items) ? 1u : 0u;
@@ -1486,7 +1503,11 @@ __global__ void __launch_bounds__(256, GSTB_LIGHT_MIN_BLOCKS) k_light(const QDev
     s_hop[i] = __ldcg(pre + T_HOP * (MAX_SLOTS + 1) + i);
   }
   __syncthreads();
+#if GSTB_STEAL
+  for (uint32_t task = warp; task < ntasks; task = next_task(&rd->next_light, nwarps, lane)) {
+#else
   for (uint32_t task = warp; task < ntasks; task += nwarps) {
+#endif
     int t = 0;
     while (t < T_HOP && task >= __ldcg(&rd->task_off[t + 1])) t++;
     const uint32_t local = task - __ldcg(&rd->task_off[t]);
@@ -1537,7 +1558,7 @@ __global__ void __launch_bounds__(256, GSTB_LIGHT_MIN_BLOCKS) k_light(const QDev
 // Heavy round kernel: the arc chunks k_light handed over this round (hub
 // vertices of distance items, high-degree DP states), then lower-bound table
 // rows (8 lanes per vertex).
-__global__ void __launch_bounds__(256, 3) k_heavy(const QDev* __restrict__ qd, const RoundDesc* __restrict__ rd,
+__global__ void __launch_bounds__(256, 3) k_heavy(const QDev* __restrict__ qd, RoundDesc* __restrict__ rd,
                                                const uint32_t* __restrict__ pre, int nslots, GraphDev g) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1559,7 +1580,11 @@ __global__ void __launch_bounds__(256, 3) k_heavy(const QDev* __restrict__ qd, c
   __syncthreads();
   const uint32_t n_lb = __ldcg(&rd->items[T_LB]), n_snap = __ldcg(&rd->items[T_SNAP]);
   const uint32_t snap0 = __ldcg(&rd->task_off[T_SNAP]);  // heavy tasks before the snapshot rows
+#if GSTB_STEAL
+  for (uint32_t task = warp; task < ntasks; task = next_task(&rd->next_heavy, nwarps, lane)) {
+#else
   for (uint32_t task = warp; task < ntasks; task += nwarps) {
+#endif
     if (task < nbig) {
       const uint4 it = __ldcg(rd->big + task);
       if (it.x & CH_GROW)
