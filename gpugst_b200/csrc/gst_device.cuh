@@ -106,7 +106,8 @@ struct alignas(64) QCtl {
   uint32_t root;
   unsigned long long best_full;  // min over full states of cost << 32 | payload
   uint32_t infeasible;  // the query groups are not connected
-  uint32_t pad0[3];
+  uint32_t center;   // hop-bounded: some vertex has every group within ceil(D/2) hops
+  uint32_t pad0[2];
   // sector 1: list append counters
   uint32_t n_near;   // append counter of the near-out list
   uint32_t n_far;    // append counter of the far list
@@ -161,6 +162,19 @@ struct QDev {
   uint32_t snap_n;   // snapshots taken (rows for b hops: snap[b-1] if b <= snap_n, else dist)
   uint32_t pad_s;
   uint32_t* snap;    // [D-1][V][8] (hop-bounded queries)
+  // Distance rows written by a distance round.  Unbounded queries relax in
+  // place (dist_nx == dist).  Hop-bounded queries run exact (Jacobi)
+  // Bellman-Ford rounds over two row buffers: round b reads dist (the exact
+  // distances over paths of at most b-1 hops) and writes dist_nx, and
+  // k_control swaps the two after the round.
+  uint32_t* dist_nx;
+  // Hop-bounded queries (D >= 2): the round whose exact rows give the
+  // incumbent (star_h = floor(D/2): a vertex with every group within star_h
+  // hops spans a tree of diameter <= D) and the round whose rows decide
+  // feasibility (center_h = ceil(D/2): every tree of diameter <= D has a
+  // vertex with every group within center_h hops).  0: none.
+  uint32_t star_h, center_h;
+  uint32_t center_done;  // the feasibility pass has run
   // progressive mode: return the best recorded tree once its cost is at most
   // ratio_num / ratio_den times the proven lower bound (ratio_num 0: exact)
   uint32_t ratio_num, ratio_den;

@@ -336,13 +336,14 @@ class Arena {
 
 // Workspace layout of one query (see gst_device.cuh).
 struct Layout {
-  size_t table, dist, dflag, qbuf, tour, lbt, snap, members, edges, total;
+  size_t table, dist, dist2, dflag, qbuf, tour, lbt, snap, members, edges, total;
   uint32_t cap;
 };
 
 // cap_req > 0 asks for a frontier-list capacity of that many items (a query
 // retried after GST_QUEUE_OVERFLOW); 0 takes the default.
-Layout layout_for(const gst_graph* g, int k, int nd, size_t n_members, uint32_t max_edges, uint64_t cap_req = 0) {
+Layout layout_for(const gst_graph* g, int k, int D, size_t n_members, uint32_t max_edges, uint64_t cap_req = 0) {
+  const int nd = D < 0 ? 1 : D + 1;
   Layout L{};
   uint64_t WT = (uint64_t)(1u << k) * nd;
   uint64_t states = (uint64_t)g->V * WT;
@@ -357,6 +358,8 @@ Layout layout_for(const gst_graph* g, int k, int nd, size_t n_members, uint32_t 
   size_t o = 0;
   L.table = o; o = align_up(o + states * 8, 256);
   L.dist = o; o = align_up(o + (size_t)g->V * 8 * 4, 256);
+  // hop-bounded queries: the second row buffer of the exact distance rounds
+  L.dist2 = o; o = align_up(o + (D >= 0 ? (size_t)g->V * 8 * 4 : 0), 256);
   L.dflag = o; o = align_up(o + ((states + 7) / 8) * 4, 256);
   L.qbuf = o; o = align_up(o + 4 * cap * 4, 256);
   L.tour = o; o = align_up(o + ((size_t)k * (1u << k) * k + (size_t)k * (1u << k) + 64) * 4, 256);
@@ -430,6 +433,7 @@ class Runner {
     CK(cudaMallocHost(&h_rd_, sizeof(RoundDesc)));
     CK(cudaMallocHost(&h_qd_, sizeof(QDev)));
     CK(cudaMallocHost(&h_one_, sizeof(uint32_t)));
+    if (env_u32("GSTB_TRACE_ROUNDS", 0)) CK(cudaMallocHost(&h_rdtrace_, 2 * 64 * sizeof(RoundDesc)));
     *h_one_ = 1u;
     // pinned staging for admissions (descriptors + member lists) and for the
     // tree read-back of retired jobs: copies from pinned memory stay
@@ -461,6 +465,8 @@ class Runner {
     if (h_rd_) cudaFreeHost(h_rd_);
     if (h_qd_) cudaFreeHost(h_qd_);
     if (h_one_) cudaFreeHost(h_one_);
+    if (h_rdtrace_) cudaFreeHost(h_rdtrace_);
+    h_rdtrace_ = nullptr;
     h_one_ = nullptr;
     if (h_stage_) cudaFreeHost(h_stage_);
     if (h_edge_stage_) cudaFreeHost(h_edge_stage_);
@@ -512,7 +518,7 @@ class Runner {
       for (uint64_t t = g_->grp_ptr[gi]; t < g_->grp_ptr[gi + 1]; t++)
         j->members.push_back(g_->grp_v[t] * 8u + (uint32_t)i);
     }
-    Layout L = layout_for(g_, j->k, j->nd, j->members.size(), max_edges_dev_, j->cap_req);
+    Layout L = layout_for(g_, j->k, j->D, j->members.size(), max_edges_dev_, j->cap_req);
     j->table_bytes = (size_t)g_->V * j->WT * 8;
     j->bytes = L.total;
     return GST_OK;
@@ -553,11 +559,12 @@ class Runner {
       }
     j->mem = (char*)p;
     j->slot = slot;
-    Layout L = layout_for(g_, j->k, j->nd, j->members.size(), max_edges_dev_, j->cap_req);
+    Layout L = layout_for(g_, j->k, j->D, j->members.size(), max_edges_dev_, j->cap_req);
     QDev& q = j->qd;
     memset(&q, 0, sizeof(q));
     q.table = (unsigned long long*)(j->mem + L.table);
     q.dist = (uint32_t*)(j->mem + L.dist);
+    q.dist_nx = j->D >= 0 ? (uint32_t*)(j->mem + L.dist2) : q.dist;
     q.dflag = (uint32_t*)(j->mem + L.dflag);
     for (int b = 0; b < 4; b++) q.qbuf[b] = (uint32_t*)(j->mem + L.qbuf) + (size_t)b * L.cap;
     q.tour = (uint32_t*)(j->mem + L.tour);
@@ -576,8 +583,13 @@ class Runner {
     q.full = (int)j->full;
     q.WT = j->WT;
     q.phase = PH_SSSP;
-    q.cap_num = cap_num_;
-    q.cap_den = cap_den_;
+    // hop-bounded queries read an unreached distance as "no path within the
+    // hops left": their distance rounds may only skip what exceeds the
+    // incumbent itself
+    q.cap_num = j->D >= 0 ? 1u : cap_num_;
+    q.cap_den = j->D >= 0 ? 1u : cap_den_;
+    q.star_h = j->D >= 2 ? (uint32_t)j->D / 2u : 0u;
+    q.center_h = j->D >= 2 ? ((uint32_t)j->D + 1u) / 2u : 0u;
     q.in_idx = 0;
     q.out_idx = 1;
     q.far_idx = 2;
@@ -595,6 +607,10 @@ class Runner {
     // distances unknown, no group pending (word FLAGW of every row)
     cudaMemsetAsync(q.dist, 0xFF, (size_t)g_->V * ROW * 4, stream_);
     cudaMemset2DAsync(q.dist + FLAGW, ROW * 4, 0, 4, g_->V, stream_);
+    if (q.dist_nx != q.dist) {
+      cudaMemsetAsync(q.dist_nx, 0xFF, (size_t)g_->V * ROW * 4, stream_);
+      cudaMemset2DAsync(q.dist_nx + FLAGW, ROW * 4, 0, 4, g_->V, stream_);
+    }
     cudaMemsetAsync(q.dflag, 0, L.qbuf - L.dflag, stream_);
     // stage the member list and both descriptors in pinned memory; it is not
     // reused before the stream synchronises at the end of the next round block
@@ -788,6 +804,9 @@ class Runner {
         if (prof) CK(cudaEventRecord(pe[3 * r + 1], stream_));
         k_heavy<<<heavy_grid_, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
         if (prof) CK(cudaEventRecord(pe[3 * r + 2], stream_));
+        if (prof && h_rdtrace_)  // the round's work counts, for the per-round trace
+          CK(cudaMemcpyAsync(h_rdtrace_ + (size_t)h * 64 + r, d_rd_, sizeof(RoundDesc), cudaMemcpyDeviceToHost,
+                             stream_));
       }
     }
     const int ns = (int)nslots_hi_;
@@ -806,6 +825,19 @@ class Runner {
       float a = 0, b = 0;
       cudaEventElapsedTime(&a, ev_prof_[h][3 * r], ev_prof_[h][3 * r + 1]);
       cudaEventElapsedTime(&b, ev_prof_[h][3 * r + 1], ev_prof_[h][3 * r + 2]);
+      if (h_rdtrace_) {
+        // GSTB_TRACE_ROUNDS: one line per profiled round: kernel times and
+        // the work of each task type (k_light: split, distance seed, DP seed,
+        // tour, extract, distance items, DP states, hop states; k_heavy:
+        // bound rows, snapshot rows; plus the arc chunks handed over)
+        const RoundDesc& d = h_rdtrace_[(size_t)h * 64 + r];
+        fprintf(stderr,
+                "gstb round %llu: light %.3f ms heavy %.3f ms | live %u | split %u sseed %u dseed %u tour %u "
+                "extract %u sssp %u (w %u) dp %u hop %u | lb %u snap %u | chunks %u%s\n",
+                (unsigned long long)g_->prof_rounds, a, b, d.n_live, d.items[T_SPLIT], d.items[T_SSEED],
+                d.items[T_DSEED], d.items[T_TOUR], d.items[T_EXTRACT], d.items[T_SSSP], d.sssp_w, d.items[T_DP],
+                d.items[T_HOP], d.items[T_LB], d.items[T_SNAP], d.n_big, d.hub_on ? " (chunking)" : "");
+      }
       g_->prof_light_ms += a;
       g_->prof_heavy_ms += b;
       g_->prof_rounds++;
@@ -865,7 +897,7 @@ class Runner {
         // a frontier outgrew its list: run the query again with 4x the capacity
         j->cap_req = std::min<uint64_t>(cap_max, (uint64_t)j->qd.cap * 4);
         j->retries++;
-        Layout L = layout_for(g_, j->k, j->nd, j->members.size(), max_edges_dev_, j->cap_req);
+        Layout L = layout_for(g_, j->k, j->D, j->members.size(), max_edges_dev_, j->cap_req);
         j->bytes = L.total;
         j->status = GST_OK;
         j->edges.clear();
@@ -905,6 +937,7 @@ class Runner {
   uint32_t blk_slots_[2] = {0, 0}, prof_rounds_[2] = {0, 0};
   cudaEvent_t ev_blk_[2] = {nullptr, nullptr}, ev_fin_ = nullptr;
   cudaEvent_t ev_prof_[2][3 * 64] = {};
+  RoundDesc* h_rdtrace_ = nullptr;  // pinned [2][64] round descriptors (GSTB_TRACE_ROUNDS)
   uint32_t delta_sssp_ = 8, delta_dp_ = 2, max_edges_dev_ = 1u << 16;
   uint32_t cap_num_ = 1, cap_den_ = 2, rounds_per_sync_ = 6;
   cudaEvent_t ev_[2] = {};
@@ -1678,7 +1711,7 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   const size_t o_pre = o;
   o = align_up(o + (size_t)NT * (MAX_SLOTS + 1) * 4, 256);
   const size_t o_ws = o;
-  Layout L = layout_for(g, k, nd, (size_t)n_members, max_edges);
+  Layout L = layout_for(g, k, D, (size_t)n_members, max_edges);
   if (o_ws + L.total > GST_NOALLOC_SCRATCH_BYTES) return GST_SCRATCH_TOO_SMALL;
 
   QDev* d_qd = reinterpret_cast<QDev*>(base + o_qd);
@@ -1691,6 +1724,7 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   memset(&q, 0, sizeof(q));
   q.table = (unsigned long long*)(ws + L.table);
   q.dist = (uint32_t*)(ws + L.dist);
+  q.dist_nx = D >= 0 ? (uint32_t*)(ws + L.dist2) : q.dist;
   q.dflag = (uint32_t*)(ws + L.dflag);
   for (int b = 0; b < 4; b++) q.qbuf[b] = (uint32_t*)(ws + L.qbuf) + (size_t)b * L.cap;
   q.tour = (uint32_t*)(ws + L.tour);
@@ -1709,8 +1743,10 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   q.full = (int)((1u << k) - 1u);
   q.WT = WT;
   q.phase = PH_SSSP;
-  q.cap_num = g->tune.cap_pct;
-  q.cap_den = 100;
+  q.cap_num = D >= 0 ? 1u : g->tune.cap_pct;
+  q.cap_den = D >= 0 ? 1u : 100u;
+  q.star_h = D >= 2 ? (uint32_t)D / 2u : 0u;
+  q.center_h = D >= 2 ? ((uint32_t)D + 1u) / 2u : 0u;
   q.in_idx = 0;
   q.out_idx = 1;
   q.far_idx = 2;
@@ -1729,6 +1765,10 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   CK(cudaMemsetAsync(q.table, 0xFF, (size_t)g->V * WT * 8, 0));
   CK(cudaMemsetAsync(q.dist, 0xFF, (size_t)g->V * ROW * 4, 0));
   CK(cudaMemset2DAsync(q.dist + FLAGW, ROW * 4, 0, 4, g->V, 0));
+  if (q.dist_nx != q.dist) {
+    CK(cudaMemsetAsync(q.dist_nx, 0xFF, (size_t)g->V * ROW * 4, 0));
+    CK(cudaMemset2DAsync(q.dist_nx + FLAGW, ROW * 4, 0, 4, g->V, 0));
+  }
   CK(cudaMemsetAsync(q.dflag, 0, L.qbuf - L.dflag, 0));
   // grids: every SM filled to the occupancy limit of each kernel
   int bl = 0, bh = 0;

@@ -28,9 +28,12 @@
 //              which its GPU path leaves commented out)
 #include "gst_device.cuh"
 
-// Round kernels take their tasks by work stealing (1) or by static striding (0).
+// Round kernels take their tasks by work stealing (1) or by static striding
+// (0, the default: on the 170k-vertex power-law workload stealing changed the
+// order of the label-correcting distance work enough to add 11% more arc
+// relaxations and ran 10% slower).
 #ifndef GSTB_STEAL
-#define GSTB_STEAL 1
+#define GSTB_STEAL 0
 #endif
 
 namespace gstb {
@@ -654,7 +657,7 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
   const uint32_t f0 = i0 == 0u ? 0u : lo_end;
   const uint32_t f1 = __shfl_sync(FULL, x, i1 - 1u);
   const uint32_t thi = q.theta_hi, nsh = near_sh(q.par ^ 1u);
-  uint32_t* __restrict__ dist = q.dist;
+  uint32_t* __restrict__ dist = q.dist_nx;  // targets: the rows this round writes
   for (uint32_t base = f0; base < f1; base += 32u * SSSP_U) {
     uint2 arc[SSSP_U];
     uint32_t itm[SSSP_U];
@@ -778,6 +781,14 @@ __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restric
       wb = __ldg(wr + 1);
     }
     const uint32_t d[KMAX] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z};
+    if (q.dist_nx != q.dist) {
+      // exact rounds: the distances that changed last round carry over into
+      // the rows this round writes (the other rows hold them already)
+      uint32_t* nx = q.dist_nx + (size_t)v * ROW;
+#pragma unroll
+      for (int t = 0; t < KMAX; t++)
+        if (t < k && ((m >> t) & 1u)) red_min(nx + t, d[t]);
+    }
     // star bound at v (unbounded queries only): v joined to every group by
     // shortest paths is a feasible tree (one-label completion, CPUNONHOP.h:684-699)
     if (q.D < 0) {
@@ -1229,6 +1240,12 @@ __device__ __forceinline__ void absorb(QDev& q, QCtl& c) {
       q.par ^= 1u;  // producers of the round flagged the next items with the other parity
       if (q.st == J_SSSP) {
         q.hops++;
+        if (q.dist_nx != q.dist) {  // exact rounds: the rows just written become the current ones
+          uint32_t* x = q.dist;
+          q.dist = q.dist_nx;
+          q.dist_nx = x;
+        }
+        if (q.hops == q.center_h + 1u) q.center_done = 1u;  // the pass ran during this round
         // rows after round b bound the paths of at most b hops: copy them
         // while the next round runs (a value it lowers in the meantime is
         // still a valid bound)
@@ -1267,6 +1284,15 @@ __device__ __forceinline__ void absorb(QDev& q, QCtl& c) {
   q.act = A_NONE;
 }
 
+// End of a hop-bounded query's distance rounds.  Every tree of hop diameter
+// <= D has a vertex with all its vertices within ceil(D/2) hops (a centre of
+// the tree), so when the exact rows of that many hops showed no vertex with
+// every group in reach, the query has no solution.
+__device__ __forceinline__ void hop_rounds_done(QDev& q, QCtl& c) {
+  if (q.center_h != 0u && q.center_done && c.center == 0u && c.best == INF32) c.infeasible = 1u;
+  q.dist_nx = q.dist;
+}
+
 __device__ __forceinline__ void decide(QDev& q, QCtl& c) {
   for (int guard = 0; guard < 8; guard++) {
     switch (q.st) {
@@ -1291,6 +1317,7 @@ __device__ __forceinline__ void decide(QDev& q, QCtl& c) {
           // and an unreached vertex cannot join a group
           q.cap1 = BIG;
           q.snap_n = min(q.hops, (uint32_t)q.D - 1u);
+          hop_rounds_done(q, c);
           q.st = J_TOUR;
           continue;
         }
@@ -1332,7 +1359,10 @@ __device__ __forceinline__ void decide(QDev& q, QCtl& c) {
         if (q.st == J_SSSP) {
           // a hop-bounded query whose rounds converged before D: rows for
           // more hops than the snapshots taken are the final distances
-          if (q.D >= 0) q.snap_n = min(q.hops, q.D > 0 ? (uint32_t)q.D - 1u : 0u);
+          if (q.D >= 0) {
+            q.snap_n = min(q.hops, q.D > 0 ? (uint32_t)q.D - 1u : 0u);
+            hop_rounds_done(q, c);
+          }
           // every distance below theta_hi is exact and every distance <=
           // cap(best) was discovered; unknown ones are >= min(theta_hi, cap+1)
           unsigned long long b1 = c.best == INF32 ? (unsigned long long)INF32 : limit + 1;
@@ -1615,6 +1645,23 @@ __global__ void __launch_bounds__(256, 3) k_heavy(const QDev* __restrict__ qd, R
       const uint4 a = __ldcg(src), b = __ldcg(src + 1);
       dst[0] = a;
       dst[1] = b;
+      if (qs.snap_h == qs.star_h || qs.snap_h == qs.center_h) {
+        // the rows are the exact distances over paths of at most snap_h hops
+        const uint32_t r[KMAX] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z};
+        bool all = true;
+        unsigned long long sum = 0;
+#pragma unroll
+        for (int t = 0; t < KMAX; t++)
+          if (t < qs.k) {
+            all = all && r[t] != INF32;
+            sum += r[t];
+          }
+        if (all && qs.snap_h == qs.center_h && __ldca(&qs.ctl->center) == 0u) atomicExch(&qs.ctl->center, 1u);
+        // v joined to every group by its cheapest path of at most star_h
+        // hops: a breadth-first tree from v inside their union has depth <=
+        // star_h, so diameter <= 2 * star_h <= D, at cost <= sum
+        if (all && qs.snap_h == qs.star_h && sum < ld_best(qs.ctl)) atomicMin(&qs.ctl->best, (uint32_t)sum);
+      }
     }
   }
   wb_flush(wb, lane);

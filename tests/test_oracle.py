@@ -100,3 +100,45 @@ def test_hop_budget_bound_keeps_the_optimum(oracle_mod):
             pruned_any += popped < ref.process
     assert checked >= 50
     assert pruned_any > 0  # the bound does cut states on these instances
+
+
+def _hop_limited(g, sources, b):
+    """Exact cheapest-path costs over paths of at most b hops from a source set
+    (Bellman-Ford rounds reading the previous round's values), numpy."""
+    INF = np.iinfo(np.int64).max // 4
+    d = np.full(g.V, INF, dtype=np.int64)
+    d[np.asarray(sources, dtype=np.int64)] = 0
+    src = np.repeat(np.arange(g.V), np.diff(g.beg_pos.astype(np.int64)))
+    for _ in range(b):
+        nd = d.copy()
+        cand = d[src] + g.weight.astype(np.int64)
+        np.minimum.at(nd, g.csr.astype(np.int64), np.where(d[src] < INF, cand, INF))
+        d = nd
+    return d, INF
+
+
+def test_hop_centre_and_star_facts(oracle_mod):
+    """The two facts the hop-bounded distance rounds rely on, checked against
+    brute force: (1) a tree of hop diameter <= D exists only if some vertex
+    has every query group within ceil(D/2) hops (a centre of the tree);
+    (2) for every vertex with all groups within floor(D/2) hops, the sum of
+    those hop-limited distances is at least the optimum (it spans a feasible
+    tree), so its minimum is a valid incumbent."""
+    O = oracle_mod
+    checked = 0
+    for g, gr, q, _ in tiny_cases(200, seed0=7000, kmax=4):
+        for D in (2, 3, 4):
+            opt = O.brute(g, gr, q, D)
+            rows_c = [_hop_limited(g, gr.group(int(j)), (D + 1) // 2) for j in q]
+            INF = rows_c[0][1]
+            centre = np.all(np.stack([r[0] < INF for r in rows_c]), axis=0).any()
+            if opt >= 0:
+                assert centre, (q.tolist(), D)
+            rows_s = [_hop_limited(g, gr.group(int(j)), D // 2)[0] for j in q]
+            st = np.stack(rows_s)
+            ok = np.all(st < INF, axis=0)
+            if ok.any():
+                star = int(st[:, ok].sum(axis=0).min())
+                assert opt >= 0 and star >= opt, (q.tolist(), D, star, opt)
+            checked += 1
+    assert checked == 600
