@@ -58,6 +58,8 @@ def load_workload(name: str):
         return g, gr, qs, [int(d) for d in z["Ds"]]
     if name == "c4":
         g, gr, qs, Ds = gen.config4()
+    elif name == "c4s":
+        g, gr, qs, Ds = gen.config4_small()
     elif name in ("c1", "c2"):
         g, gr, per_k = gen.config1() if name == "c1" else gen.config2()
         ks = sorted(per_k)
@@ -78,6 +80,9 @@ def workload_desc(name):
     if name == "c4":
         return ("chung-lu V=3000000 E=117M gamma=2.1 w~U[1,100]; 1000000 zipf(1.3) groups in [1,500]; "
                 "1024 queries k~U{3..6}, half with D~U{2,3,4}")
+    if name == "c4s":
+        return ("chung-lu V=1000000 E=39M gamma=2.1 w~U[1,100]; 333333 zipf(1.3) groups in [1,500]; "
+                "1024 queries k~U{3..6}, half with D~U{2,3,4} (the batched configuration at a third of its size)")
     if name == "c2":
         return ("chung-lu V=170000 E=6.8M gamma=2.3 w~U[1,100]; 200000 zipf(1.5) groups in [1,200]; "
                 "queries k=3,4,5 interleaved (300 each)")
@@ -217,7 +222,7 @@ def cpu_baseline_port(g, gr, qs, Ds, workload):
     from oracle import oracle
     oracle.build()
     cores = max(1, min(os.cpu_count() or 1, 32))
-    if workload == "c4":
+    if workload in ("c4", "c4s"):
         # unbounded k = 3 queries: the restatement takes about 30 s each on
         # this graph (k = 6 takes minutes)
         sample = [i for i in range(len(qs)) if Ds[i] < 0 and len(qs[i]) == 3][:cores]
@@ -283,7 +288,7 @@ def run_reference(args, g, gr, qs, Ds, rank, world):
     if not os.path.exists(ref_bin):
         raise SystemExit("oracle/_ref/prunedpp_ref missing: build it with make -C oracle ref")
     nproc = os.cpu_count() or 1
-    big = args.workload == "c4"
+    big = args.workload in ("c4", "c4s")
     try:
         import psutil
         per_proc = (16 << 30) if big else (3 << 30)
@@ -411,7 +416,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c1"])
+    ap.add_argument("--workload", default="c4", choices=["c4", "c4s", "c2", "c1"])
     ap.add_argument("--batch", type=int, default=0, help="queries per step (default: 128 on c4, 90 on c2)")
     ap.add_argument("--plain", type=int, default=300, help="queries on the plain per-query path")
     ap.add_argument("--sweep", default="1,2,4,8,16,32", help="closed-loop serving concurrencies")
@@ -422,7 +427,7 @@ def main():
     ap.add_argument("--c5-drain", type=float, default=5.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
-    big = args.workload == "c4"
+    big = args.workload in ("c4", "c4s")
     B = args.batch or (128 if big else 90)
     n_sweep = args.sweep_queries or (64 if big else 256)
 

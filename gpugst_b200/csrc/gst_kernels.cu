@@ -224,6 +224,27 @@ __device__ __forceinline__ void push_multi(bool take, uint32_t item, uint32_t wh
   }
 }
 
+// Hop-bounded queries: the largest distance from vertex u to a group of comp
+// over paths of at most b hops (INF32 if one is out of reach), computed by
+// one lane for its own u.  Rows for b hops are the snapshot after round b
+// while snapshots were taken, else the final rows; for b = 0 only u itself
+// counts (distance 0: u is a member).
+__device__ __forceinline__ uint32_t hop_budget_one(const QDev& q, uint32_t u, uint32_t comp, uint32_t b) {
+  const uint32_t* row = (b >= 1u && b <= q.snap_n) ? q.snap + ((size_t)(b - 1u) * q.nv + u) * ROW
+                                                   : q.dist + (size_t)u * ROW;
+  const uint4* r4 = reinterpret_cast<const uint4*>(row);
+  const uint4 x = __ldcg(r4), y = __ldcg(r4 + 1);
+  const uint32_t r[KMAX] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z};
+  uint32_t mx = 0;
+#pragma unroll
+  for (int j = 0; j < KMAX; j++)
+    if (j < q.k && ((comp >> j) & 1u)) {
+      const uint32_t d = b == 0u ? (r[j] == 0u ? 0u : INF32) : r[j];
+      mx = max(mx, d);
+    }
+  return mx;
+}
+
 // ---------------------------------------------------------------------------
 // Grow of one DP state (v, p) -- or (v, p, d) with target hop count d+1 --
 // along its arcs [a0, a1): target (u, p[, d+1]) at cost c + w(v, u).  GROW_U
@@ -273,6 +294,20 @@ __device__ __forceinline__ void grow_arcs(const QDev& q, const GraphDev& g, uint
       nc[u] = c + arc[u].y;
       want[u] = ok[u] && nc[u] < cur[u] && lb_ok(nc[u], lbu[u], best);
       if (ok[u]) cnt.arcs++;
+    }
+    if (dnext >= 0) {
+      // hop-bounded target (u, p, dnext): its missing groups must stay within
+      // the D - dnext hops left from u (the test its expansion would apply);
+      // a target that fails is never written, flagged or queued
+#pragma unroll
+      for (int u = 0; u < GROW_U; u++)
+        if (want[u]) {
+          const uint32_t h = hop_budget_one(q, arc[u].x, comp, (uint32_t)(q.D - dnext));
+          want[u] = h != INF32 && (unsigned long long)nc[u] + h <= best;
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < GROW_U; u++) {
       if (want[u]) {
         // the pre-check already saw a higher cost: enqueue on it and let the
         // 64-bit min land without waiting for its result (a concurrent lower
@@ -340,61 +375,96 @@ __device__ __forceinline__ void load_dl(const QDev& q, uint32_t v, uint32_t (&dl
   }
 }
 
+// Slot owning flat item `it` of task type t: largest s with pre[s] <= it.
+__device__ __forceinline__ uint32_t find_slot(const uint32_t* __restrict__ pre, int nslots, uint32_t it) {
+  int lo = 0, hi = nslots;  // pre[lo] <= it < pre[hi]
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (__ldcg(pre + mid) <= it)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return (uint32_t)lo;
+}
+
+// Same search over a prefix array staged in shared memory.
+__device__ __forceinline__ uint32_t find_slot_s(const uint32_t* pre, int nslots, uint32_t it) {
+  int lo = 0, hi = nslots;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (pre[mid] <= it)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return (uint32_t)lo;
+}
+
 // ---------------------------------------------------------------------------
-// Unbounded DP item (v, p).
+// Unbounded DP item (v, p), in two parts.  dp_gate runs on one lane for its
+// own item: it takes the item out of the near list, drops it when its cost
+// is above the incumbent, updates the incumbent from the complement merge
+// and the one-label completion, and applies the bound; dp_expand then grows
+// and merges the surviving state with the whole warp.
 // ---------------------------------------------------------------------------
-__device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t lane, RoundDesc* __restrict__ rd,
-                        uint32_t slot, WarpStat& ws, WarpBuf& wb) {
-  const unsigned FULL = 0xFFFFFFFFu;
+__device__ __forceinline__ bool dp_gate(const QDev& q, uint32_t s, uint32_t& c_out, uint32_t& best_out,
+                                        bool& counted) {
   const int k = q.k;
   const uint32_t K2 = 1u << k, full = (uint32_t)q.full;
   const uint32_t v = s >> k, p = s & (K2 - 1u);
-  if (lane == 0) atomicAnd(&q.dflag[s >> 3], ~dflag_bit(s, q.par));
-  __syncwarp();
-  uint32_t c = __shfl_sync(FULL, (uint32_t)(ld_cg(q.table + s) >> 32), 0);
-  uint32_t best = __shfl_sync(FULL, ld_best(q.ctl), 0);
-  if (c == INF32 || c > best) return;
+  counted = false;
+  atomicAnd(&q.dflag[s >> 3], ~dflag_bit(s, q.par));
+  const uint32_t c = (uint32_t)(ld_cg(q.table + s) >> 32);
+  uint32_t best = ld_best(q.ctl);
+  if (c == INF32 || c > best) return false;
   unsigned long long* row = q.table + (size_t)v * K2;
   if (p == full) {
-    if (lane == 0 && c < best) atomicMin(&q.ctl->best, c);
-    return;
+    if (c < best) atomicMin(&q.ctl->best, c);
+    return false;
   }
   const uint32_t comp = full ^ p;
   uint32_t dl[KMAX], sum_ok;
   unsigned long long raw_sum;
   load_dl(q, v, dl, sum_ok, comp, raw_sum);
-  if (lane == 0) {
-    // complement merge straight into the full state (DPQ.cu:82-94); a full
-    // state of cost equal to best is still recorded: best may come from a
-    // bound-only tree (star or one-label) that has no table entry
-    uint32_t cc = (uint32_t)(ld_cg(row + comp) >> 32);
-    if (cc != INF32) {
-      unsigned long long m = (unsigned long long)c + cc;
-      if (m <= best) {
-        atomicMin(row + full, pack((uint32_t)m, PAR_MERGE | p));
-        atomicMin(&q.ctl->best_full, (m << 32) | v);
-        if (m < best) {
-          atomicMin(&q.ctl->best, (uint32_t)m);
-          best = (uint32_t)m;
-        }
+  // complement merge straight into the full state (DPQ.cu:82-94); a full
+  // state of cost equal to best is still recorded: best may come from a
+  // bound-only tree (star or one-label) that has no table entry
+  const uint32_t cc = (uint32_t)(ld_cg(row + comp) >> 32);
+  if (cc != INF32) {
+    const unsigned long long m = (unsigned long long)c + cc;
+    if (m <= best) {
+      atomicMin(row + full, pack((uint32_t)m, PAR_MERGE | p));
+      atomicMin(&q.ctl->best_full, (m << 32) | v);
+      if (m < best) {
+        atomicMin(&q.ctl->best, (uint32_t)m);
+        best = (uint32_t)m;
       }
     }
-    // one-label completion: T(v,p) plus shortest paths to the missing groups
-    // (DPQ.cu:95-107, CPUNONHOP.h:684-699)
-    if (sum_ok) {
-      unsigned long long ol = (unsigned long long)c + raw_sum;
-      if (ol < best) {
-        atomicMin(&q.ctl->best, (uint32_t)ol);
-        best = (uint32_t)ol;
-      }
-    }
-    ws_add(ws, q.ctl, ST_EXPANDED, 1u);
   }
-  best = __shfl_sync(FULL, best, 0);
-  const unsigned short* lbt = q.lbt;
-  uint32_t lbv = __ldg(lbt + ((size_t)v << k) + comp);
-  if (!lb_ok(c, lbv, best)) return;
+  // one-label completion: T(v,p) plus shortest paths to the missing groups
+  // (DPQ.cu:95-107, CPUNONHOP.h:684-699)
+  if (sum_ok) {
+    const unsigned long long ol = (unsigned long long)c + raw_sum;
+    if (ol < best) {
+      atomicMin(&q.ctl->best, (uint32_t)ol);
+      best = (uint32_t)ol;
+    }
+  }
+  counted = true;
+  const uint32_t lbv = __ldg(q.lbt + ((size_t)v << k) + comp);
+  c_out = c;
+  best_out = best;
+  return lb_ok(c, lbv, best);
+}
 
+__device__ void dp_expand(const QDev& q, const GraphDev& g, uint32_t s, uint32_t c, uint32_t best, uint32_t lane,
+                          RoundDesc* __restrict__ rd, uint32_t slot, WarpStat& ws, WarpBuf& wb) {
+  const int k = q.k;
+  const uint32_t K2 = 1u << k, full = (uint32_t)q.full;
+  const uint32_t v = s >> k, p = s & (K2 - 1u), comp = full ^ p;
+  unsigned long long* row = q.table + (size_t)v * K2;
+  const unsigned short* lbt = q.lbt;
   GrowCnt gc;
   // grow, only from states of cost <= best/2 (optimal-tree decomposition,
   // CPUNONHOP.h:820; exact for the unbounded problem); a high-degree vertex
@@ -450,63 +520,49 @@ __device__ void dp_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t l
   }
 }
 
-// Hop-bounded queries: lower bound of joining every group of comp to v
-// within b hops, INF32 if one is out of reach.  In a derivation of a tree of
-// hop diameter <= D from state (v, p, d), a group missing from p is reached
-// from v by a path outside the subtree, and that path plus the subtree's
-// height d is a path of the tree: it has at most D - d hops.  Rows for b hops
-// are the snapshot after Bellman-Ford round b (or the final rows once the
-// rounds stopped); for b = 0 only v itself counts (distance 0: v is in the
-// group).  Every lane calls it; lanes j < k read word j of the row.
-__device__ __forceinline__ uint32_t hop_budget_lb(const QDev& q, uint32_t v, uint32_t comp, uint32_t b,
-                                                  uint32_t lane) {
-  const uint32_t* row = (b >= 1u && b <= q.snap_n) ? q.snap + ((size_t)(b - 1u) * q.nv + v) * ROW
-                                                   : q.dist + (size_t)v * ROW;
-  uint32_t x = 0;
-  if (lane < (uint32_t)q.k && ((comp >> lane) & 1u)) {
-    x = __ldcg(row + lane);
-    if (b == 0u) x = x == 0u ? 0u : INF32;
-  }
-#pragma unroll
-  for (int o = 4; o > 0; o >>= 1) x = max(x, __shfl_xor_sync(0xFFFFFFFFu, x, o));
-  return __shfl_sync(0xFFFFFFFFu, x, 0);
-}
-
 // ---------------------------------------------------------------------------
-// Hop-bounded DP item (v, p, d): state id ((v << k) | p) * nd + d.
+// Hop-bounded DP item (v, p, d): state id ((v << k) | p) * nd + d; gate on
+// one lane, expansion by the warp, as for the unbounded items.
 // ---------------------------------------------------------------------------
-__device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t lane, RoundDesc* __restrict__ rd,
-                         uint32_t slot, WarpStat& ws, WarpBuf& wb) {
-  const unsigned FULL = 0xFFFFFFFFu;
+__device__ __forceinline__ bool hop_gate(const QDev& q, uint32_t s, uint32_t& c_out, uint32_t& best_out,
+                                         bool& counted) {
   const int k = q.k, nd = q.nd, D = q.D;
   const uint32_t K2 = 1u << k, full = (uint32_t)q.full;
   const uint32_t d = s % (uint32_t)nd, vp = s / (uint32_t)nd;
   const uint32_t v = vp >> k, p = vp & (K2 - 1u);
-  if (lane == 0) atomicAnd(&q.dflag[s >> 3], ~dflag_bit(s, q.par));
-  __syncwarp();
-  uint32_t c = __shfl_sync(FULL, (uint32_t)(ld_cg(q.table + s) >> 32), 0);
-  uint32_t best = __shfl_sync(FULL, ld_best(q.ctl), 0);
-  if (c == INF32 || c > best) return;
+  counted = false;
+  atomicAnd(&q.dflag[s >> 3], ~dflag_bit(s, q.par));
+  const uint32_t c = (uint32_t)(ld_cg(q.table + s) >> 32);
+  const uint32_t best = ld_best(q.ctl);
+  if (c == INF32 || c > best) return false;
   // dominance: the same subset at a smaller hop count and no higher cost
-  {
-    bool dom = false;
-    if (lane < d) dom = (uint32_t)(ld_cg(q.table + (size_t)vp * nd + lane) >> 32) <= c;
-    if (__any_sync(FULL, dom)) return;
-  }
+  for (uint32_t e = 0; e < d; e++)
+    if ((uint32_t)(ld_cg(q.table + (size_t)vp * nd + e) >> 32) <= c) return false;
   if (p == full) {
-    if (lane == 0 && c < best) atomicMin(&q.ctl->best, c);
-    return;
+    if (c < best) atomicMin(&q.ctl->best, c);
+    return false;
   }
   const uint32_t comp = full ^ p;
-  {
-    // the missing groups within the hops left (D - d) of v
-    const uint32_t lbh = hop_budget_lb(q, v, comp, (uint32_t)D - d, lane);
-    if (lbh == INF32 || (unsigned long long)c + lbh > best) return;
-  }
-  if (lane == 0) ws_add(ws, q.ctl, ST_EXPANDED, 1u);
+  // In a derivation of a tree of hop diameter <= D from (v, p, d), a group
+  // missing from p is reached from v by a path outside the subtree, and that
+  // path plus the subtree's height d is a path of the tree: it has at most
+  // D - d hops.  So the missing groups must be within D - d hops of v.
+  const uint32_t lbh = hop_budget_one(q, v, comp, (uint32_t)D - d);
+  if (lbh == INF32 || (unsigned long long)c + lbh > best) return false;
+  counted = true;
+  const uint32_t lbv = __ldg(q.lbt + ((size_t)v << k) + comp);
+  c_out = c;
+  best_out = best;
+  return lb_ok(c, lbv, best);
+}
+
+__device__ void hop_expand(const QDev& q, const GraphDev& g, uint32_t s, uint32_t c, uint32_t best, uint32_t lane,
+                           RoundDesc* __restrict__ rd, uint32_t slot, WarpStat& ws, WarpBuf& wb) {
+  const int k = q.k, nd = q.nd, D = q.D;
+  const uint32_t K2 = 1u << k, full = (uint32_t)q.full;
+  const uint32_t d = s % (uint32_t)nd, vp = s / (uint32_t)nd;
+  const uint32_t v = vp >> k, p = vp & (K2 - 1u), comp = full ^ p;
   const unsigned short* lbt = q.lbt;
-  uint32_t lbv = __ldg(lbt + ((size_t)v << k) + comp);
-  if (!lb_ok(c, lbv, best)) return;
   GrowCnt gc;
   if (d < (uint32_t)D) {  // grow d -> d+1 (CPUHOP.h:192-206)
     const uint32_t lim = best - c;
@@ -571,6 +627,47 @@ __device__ void hop_item(const QDev& q, const GraphDev& g, uint32_t s, uint32_t 
   }
 }
 
+// A DP task: W items (one per lane) of the round's DP or hop-bounded list.
+// Each lane runs its item's gates; then the warp expands the surviving
+// states one after another.  W is chosen per round by k_control (1 when the
+// round has few items, so that each state gets a warp of its own; up to 32
+// when it has many, most of which the gates drop).
+__device__ void dp_task(const QDev* __restrict__ qd, const uint32_t* __restrict__ pre, int nslots, uint32_t total,
+                        uint32_t task, uint32_t W, bool hop, const GraphDev& g, uint32_t lane,
+                        RoundDesc* __restrict__ rd, WarpStat& ws, WarpBuf& wb) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  const uint32_t it = task * W + lane;
+  const bool valid = lane < W && it < total;
+  uint32_t slot = 0xFFFFFFFFu, s = 0, c = 0, best = 0;
+  bool live = false, counted = false;
+  if (valid) {
+    slot = find_slot_s(pre, nslots, it);
+    const QDev& q = qd[slot];
+    s = q.qbuf[q.in_idx][it - pre[slot]];
+    live = hop ? hop_gate(q, s, c, best, counted) : dp_gate(q, s, c, best, counted);
+  }
+  // expanded-state counts, per query of the task
+  unsigned cm = __ballot_sync(FULL, counted);
+  while (cm) {
+    const uint32_t si = __shfl_sync(FULL, slot, __ffs(cm) - 1);
+    const unsigned same = __ballot_sync(FULL, counted && slot == si);
+    if (lane == 0) ws_add(ws, qd[si].ctl, ST_EXPANDED, __popc(same));
+    cm &= ~same;
+  }
+  unsigned lm = __ballot_sync(FULL, live);
+  while (lm) {
+    const uint32_t i = __ffs(lm) - 1;
+    lm &= lm - 1u;
+    const uint32_t si = __shfl_sync(FULL, slot, i), ss = __shfl_sync(FULL, s, i);
+    const uint32_t cc = __shfl_sync(FULL, c, i), bb = __shfl_sync(FULL, best, i);
+    const QDev& q = qd[si];
+    if (hop)
+      hop_expand(q, g, ss, cc, bb, lane, rd, si, ws, wb);
+    else
+      dp_expand(q, g, ss, cc, bb, lane, rd, si, ws, wb);
+  }
+}
+
 // Next task of a warp.  Each warp's first task is its own index; after that
 // the warps take tasks from a shared counter (work stealing), so a warp that
 // met cheap tasks keeps taking new ones while one with a long task (a hub
@@ -579,32 +676,6 @@ __device__ __forceinline__ uint32_t next_task(uint32_t* counter, uint32_t nwarps
   uint32_t t = 0;
   if (lane == 0) t = nwarps + atomicAdd(counter, 1u);
   return __shfl_sync(0xFFFFFFFFu, t, 0);
-}
-
-// Slot owning flat item `it` of task type t: largest s with pre[s] <= it.
-__device__ __forceinline__ uint32_t find_slot(const uint32_t* __restrict__ pre, int nslots, uint32_t it) {
-  int lo = 0, hi = nslots;  // pre[lo] <= it < pre[hi]
-  while (hi - lo > 1) {
-    int mid = (lo + hi) >> 1;
-    if (__ldcg(pre + mid) <= it)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  return (uint32_t)lo;
-}
-
-// Same search over a prefix array staged in shared memory.
-__device__ __forceinline__ uint32_t find_slot_s(const uint32_t* pre, int nslots, uint32_t it) {
-  int lo = 0, hi = nslots;
-  while (hi - lo > 1) {
-    int mid = (lo + hi) >> 1;
-    if (pre[mid] <= it)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  return (uint32_t)lo;
 }
 
 // ---------------------------------------------------------------------------
@@ -658,6 +729,13 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
   const uint32_t f1 = __shfl_sync(FULL, x, i1 - 1u);
   const uint32_t thi = q.theta_hi, nsh = near_sh(q.par ^ 1u);
   uint32_t* __restrict__ dist = q.dist_nx;  // targets: the rows this round writes
+  // Exact (Jacobi) rounds compare against the target's row of the previous
+  // round: the value the round must beat.  The written row can still hold
+  // the value of two rounds ago for a vertex that changed last round and has
+  // not copied its new value across yet; a comparison with it would write
+  // and flag non-improvements.
+  const bool jac = q.dist_nx != q.dist;
+  const uint32_t* __restrict__ prev = jac ? q.dist : q.dist_nx;
   for (uint32_t base = f0; base < f1; base += 32u * SSSP_U) {
     uint2 arc[SSSP_U];
     uint32_t itm[SSSP_U];
@@ -685,7 +763,7 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
     for (int u = 0; u < SSSP_U; u++) {
       ok[u] = ok[u] && arc[u].y <= h[itm[u]].lim;
       if (ok[u]) {
-        const uint4* row = reinterpret_cast<const uint4*>(dist + (size_t)arc[u].x * 8);
+        const uint4* row = reinterpret_cast<const uint4*>(prev + (size_t)arc[u].x * 8);
         ra[u] = __ldcg(row);
         rb[u] = __ldcg(row + 1);
       } else {
@@ -731,8 +809,14 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
 #pragma unroll
     for (int u = 0; u < SSSP_U; u++) {
       const uint32_t bits = (nn[u] << nsh) | (nf[u] << FAR_SH);
-      const uint32_t fw = rb[u].w;
-      if (bits & ~fw) red_or(dist + (size_t)arc[u].x * ROW + FLAGW, bits);
+      uint32_t fw = rb[u].w;
+      if (jac) {
+        // the row read was the previous round's: the flags of the written
+        // row come back from the OR itself
+        fw = bits ? atomicOr(dist + (size_t)arc[u].x * ROW + FLAGW, bits) : bits;
+      } else if (bits & ~fw) {
+        red_or(dist + (size_t)arc[u].x * ROW + FLAGW, bits);
+      }
       tN[u] = nn[u] && ((fw >> nsh) & 0xFFu) == 0u;
       tF[u] = nf[u] && ((fw >> FAR_SH) & 0xFFu) == 0u;
       itv[u] = arc[u].x;
@@ -1096,26 +1180,70 @@ __device__ void tour_warp(const QDev& q, uint32_t lane) {
   __syncwarp();
 }
 
-// Lower-bound table row of vertex v: lbt[v][X] = lower_bound_comp(d(v), X)
-// for every subset X (the per-vertex one_label_lb table of the reference,
-// DPQ.cu:174-224, with the tour bounds of CPUNONHOP.h:436-496).  Eight lanes
-// share a vertex and split its subsets.  Saturated to 16 bits, which only
-// lowers a bound.
-__device__ void lbt_row8(const QDev& q, uint32_t v, uint32_t sl) {
-  const int k = q.k;
-  const uint32_t K2 = 1u << k;
-  const uint32_t* P = q.tour;
-  const uint32_t* T2 = q.tour + (size_t)k * K2 * k;
-  const uint4* row = reinterpret_cast<const uint4*>(q.dist + (size_t)v * 8);
-  uint4 a = __ldg(row), b = __ldg(row + 1);
-  uint32_t r[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-  uint32_t dl[KMAX];
+// Lower-bound table rows: lbt[v][X] = lower_bound_comp(d(v), X) for every
+// subset X (the per-vertex one_label_lb table of the reference,
+// DPQ.cu:174-224, with the tour bounds of CPUNONHOP.h:436-496), saturated to
+// 16 bits, which only lowers a bound.  32 consecutive items, one vertex per
+// lane.  All lanes evaluate the same subset X at a time, so the bound's
+// loops over the groups of X branch alike in every lane and the tour-table
+// reads are one broadcast per warp; each lane packs 8 entries of its row
+// into one 16-byte store.  Items of different
+// queries in one task are handled run by run.
+__device__ void lbt_rows32(const QDev* __restrict__ qd, const uint32_t* __restrict__ pre, int nslots, uint32_t n_lb,
+                           uint32_t task, uint32_t lane) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  const uint32_t it = task * 32u + lane;
+  const bool valid = it < n_lb;
+  const uint32_t slot = valid ? find_slot_s(pre, nslots, it) : 0xFFFFFFFFu;
+  const uint32_t prev = __shfl_up_sync(FULL, slot, 1);
+  unsigned runs = __ballot_sync(FULL, valid && (lane == 0u || prev != slot));
+  while (runs) {
+    const uint32_t i0 = (uint32_t)(__ffs(runs) - 1);
+    runs &= runs - 1u;
+    const uint32_t si = __shfl_sync(FULL, slot, i0);
+    const bool mine = valid && slot == si;
+    const QDev& q = qd[si];
+    const int k = q.k;
+    const uint32_t K2 = 1u << k;
+    const uint32_t* P = q.tour;
+    const uint32_t* T2 = q.tour + (size_t)k * K2 * k;
+    const uint32_t v = mine ? q.lb_off + (it - pre[si]) : 0u;
+    uint32_t dl[KMAX];
+    {
+      uint4 a = make_uint4(0u, 0u, 0u, 0u), b = a;
+      if (mine) {
+        const uint4* row = reinterpret_cast<const uint4*>(q.dist + (size_t)v * ROW);
+        a = __ldg(row);
+        b = __ldg(row + 1);
+      }
+      const uint32_t r[KMAX] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z};
 #pragma unroll
-  for (int j = 0; j < KMAX; j++) dl[j] = min(r[j], q.cap1);
-  unsigned short* out = q.lbt + ((size_t)v << k);
-  for (uint32_t X = sl; X < K2; X += 8) {
-    const uint32_t lb = X == 0 ? 0u : lower_bound_comp(dl, k, X, P, T2);
-    out[X] = (unsigned short)(lb >= BIG ? LB_INF : min(lb, LB_INF - 1u));
+      for (int j = 0; j < KMAX; j++) dl[j] = min(r[j], q.cap1);
+    }
+    unsigned short* out = q.lbt + ((size_t)v << k);
+    for (uint32_t x0 = 0; x0 < K2; x0 += 8u) {
+      uint32_t pk[4];
+#pragma unroll
+      for (int h = 0; h < 4; h++) {
+        uint32_t two = 0;
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const uint32_t X = x0 + 2u * h + e;
+          uint32_t lb = 0;
+          if (X != 0u && X < K2) lb = lower_bound_comp(dl, k, X, P, T2);
+          const uint32_t ent = lb >= BIG ? LB_INF : min(lb, LB_INF - 1u);
+          two |= ent << (16 * e);
+        }
+        pk[h] = two;
+      }
+      if (mine) {
+        if (K2 >= 8u) {
+          *reinterpret_cast<uint4*>(out + x0) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        } else {
+          for (uint32_t X = 0; X < K2; X++) out[X] = (unsigned short)(pk[X >> 1] >> (16 * (X & 1u)));
+        }
+      }
+    }
   }
 }
 
@@ -1477,7 +1605,15 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
     const unsigned long long n_sssp = wsum[(blockDim.x >> 5) - 1][T_SSSP];
     while (w < SSSP_WMAX && n_sssp > 2ull * w * rd->light_warps) w <<= 1;
     rd->sssp_w = w;
-    const uint32_t per_task[NT] = {32, 32, 32, 1, 1, w, 1, 1, 4, 32};
+    // DP states per warp task: 1 while that leaves at most two tasks per
+    // light warp (every state gets a warp), more (up to 32) in rounds with
+    // many states
+    uint32_t wd = 1;
+    const unsigned long long n_dp = (unsigned long long)wsum[(blockDim.x >> 5) - 1][T_DP] +
+                                    wsum[(blockDim.x >> 5) - 1][T_HOP];
+    while (wd < 32u && n_dp > 2ull * wd * rd->light_warps) wd <<= 1;
+    rd->dp_w = wd;
+    const uint32_t per_task[NT] = {32, 32, 32, 1, 1, w, wd, wd, 32, 32};
     uint32_t off = 0;
     for (int t = 0; t < NT; t++) {
       uint32_t tot = wsum[(blockDim.x >> 5) - 1][t];
@@ -1546,14 +1682,8 @@ __global__ void __launch_bounds__(256, GSTB_LIGHT_MIN_BLOCKS) k_light(const QDev
     if (t == T_SSSP) {
       sssp_task(qd, s_pre, nslots, total, local, __ldcg(&rd->sssp_w), g, lane, ws, rd, s_hdr[threadIdx.x >> 5], wb);
     } else if (t == T_DP || t == T_HOP) {
-      const uint32_t* S = t == T_DP ? s_dp : s_hop;
-      const uint32_t slot = find_slot_s(S, nslots, local);
-      const QDev& q = qd[slot];
-      const uint32_t st = q.qbuf[q.in_idx][local - S[slot]];
-      if (t == T_DP)
-        dp_item(q, g, st, lane, rd, slot, ws, wb);
-      else
-        hop_item(q, g, st, lane, rd, slot, ws, wb);
+      dp_task(qd, t == T_DP ? s_dp : s_hop, nslots, total, local, __ldcg(&rd->dp_w), t == T_HOP, g, lane, rd, ws,
+              wb);
     } else if (t == T_TOUR) {
       tour_warp(qd[find_slot(P, nslots, local)], lane);
     } else if (t == T_EXTRACT) {
@@ -1624,13 +1754,8 @@ __global__ void __launch_bounds__(256, 3) k_heavy(const QDev* __restrict__ qd, R
       continue;
     }
     const uint32_t ht = task - nbig;
-    if (ht < snap0) {  // lower-bound table rows, 8 lanes per vertex
-      const uint32_t it = ht * 4u + (lane >> 3);
-      if (it < n_lb) {
-        const uint32_t slot = find_slot_s(s_lb, nslots, it);
-        const QDev& ql = qd[slot];
-        lbt_row8(ql, ql.lb_off + (it - s_lb[slot]), lane & 7u);
-      }
+    if (ht < snap0) {  // lower-bound table rows, one vertex per lane
+      lbt_rows32(qd, s_lb, nslots, n_lb, ht, lane);
       continue;
     }
     // snapshot of a hop-bounded query's distance rows, one row per lane

@@ -285,6 +285,22 @@ def config4(seed: int = 4, n_queries: int = 1024):
     return g, gr, qs, Ds
 
 
+def config4_small(seed: int = 4, n_queries: int = 1024):
+    """The batched configuration at a third of its size, for profiler
+    captures that must stay within a few GB of device memory: V=1M, E=39M
+    Chung-Lu (gamma 2.1); 333,333 Zipf(1.3) groups in [1,500]; 1,024 queries,
+    k uniform in {3,4,5,6}, half with D uniform in {2,3,4}."""
+    g = chung_lu(1_000_000, 39_000_000, 2.1, seed=1100 + seed)
+    gr = zipf_groups(g.V, 333_333, 1.3, 500, seed=2100 + seed)
+    rng = np.random.default_rng(3100 + seed)
+    qs, Ds = [], []
+    for _ in range(n_queries):
+        k = int(rng.integers(3, 7))
+        qs.append(rng.choice(gr.n_groups, size=k, replace=False).astype(np.uint32))
+        Ds.append(int(rng.choice([2, 3, 4])) if rng.random() < 0.5 else -1)
+    return g, gr, qs, Ds
+
+
 def poisson_arrivals(rate: float, duration: float, seed: int) -> np.ndarray:
     """Arrival times (seconds) of a Poisson process of the given rate."""
     rng = np.random.default_rng(seed)
