@@ -65,8 +65,10 @@ struct RoundDesc {
   uint32_t hub_min_rest;  // ... and only when at least this many arcs remain under the limit
   uint32_t hub_max_items; // chunk only in rounds with fewer distance items (latency-bound rounds)
   uint32_t hub_on;        // set by k_control for the current round
+  uint32_t grow_chunks;   // DP grows hand hub arcs out this round (set by k_control)
   uint32_t sssp_w;        // distance items per warp task this round (set by k_control)
   uint32_t dp_w;          // DP states per warp task this round (set by k_control)
+  uint32_t dp_wmax;       // largest DP task width (set by the host)
   uint32_t light_warps;   // warps of one k_light launch (set by the host)
   uint32_t nslots;        // 1 + the highest slot in use this round (set by k_control)
   // work stealing: a warp that finished its first task takes the next one

@@ -413,7 +413,7 @@ class Runner {
     }
     {
       // hub arc chunk list (k_light -> k_heavy within a round)
-      big_cap_ = std::max(1u << 12, env_u32("GSTB_HUB_CHUNKS", 1u << 20));
+      big_cap_ = std::max(1u << 12, env_u32("GSTB_HUB_CHUNKS", 1u << 22));
       CK(cudaMalloc(&d_big_, (size_t)big_cap_ * sizeof(uint4)));
       RoundDesc rd;
       memset(&rd, 0, sizeof(rd));
@@ -424,6 +424,7 @@ class Runner {
       rd.hub_max_items = env_u32("GSTB_HUB_MAX_ITEMS", 1000000);
       rd.light_warps = light_grid_ * (256 / 32);
       rd.sssp_w = 4;
+      rd.dp_wmax = std::min(32u, std::max(1u, env_u32("GSTB_DP_WMAX", 32)));
       CK(cudaMemcpy(d_rd_, &rd, sizeof(rd), cudaMemcpyHostToDevice));
     }
     CK(cudaMalloc(&d_pre_, (size_t)NT * (MAX_SLOTS + 1) * 4));
@@ -1297,13 +1298,15 @@ gst_status gst_query_batch_ratio(gst_graph* g, int n, const uint32_t* groups, co
       },
       [&](Job*) {});
   if (rs != GST_OK) return rs;
-  // a large batch's workspaces go back to the device (serving loops and
-  // other engines allocate their own) once the arena holds more than
-  // GSTB_ARENA_KEEP_MB, by default a quarter of the device's memory
+  // The arena keeps its chunks for the next batch (handing them back and
+  // allocating them again cost a cudaFree / cudaMalloc pair per batch).
+  // GSTB_ARENA_KEEP_MB caps what it keeps; a serving loop opened on this
+  // graph takes back the wholly free chunks first (gst_serve_open).
   {
     const uint32_t keep_mb = env_u32("GSTB_ARENA_KEEP_MB", 0);
-    R.release_arena_above(keep_mb ? (size_t)keep_mb << 20 : g->total_mem / 4);
+    if (keep_mb) R.release_arena_above((size_t)keep_mb << 20);
   }
+
   const clk::time_point t2 = clk::now();
   for (int i = 0; i < n; i++) {
     Job& j = jobs[i];
@@ -1472,6 +1475,12 @@ extern "C" {
 gst_status gst_serve_open(gst_graph* g, uint64_t hbm_budget_bytes, int max_inflight, gst_server** out) {
   if (!g || !out || !has_groups(g)) return GST_BAD_INPUT;
   *out = nullptr;
+  {
+    // the batch engine of this graph gives back its wholly free workspace
+    // chunks, which the serving loop's own arena may need
+    std::lock_guard<std::mutex> lock(g->mu);
+    if (g->runner) static_cast<Runner*>(g->runner)->release_arena_above(0);
+  }
   gst_server* S = new gst_server();
   S->g = g;
   S->runner = new Runner(g);
@@ -1781,6 +1790,7 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
     memset(&rd0, 0, sizeof(rd0));
     rd0.light_warps = light_grid * (256 / 32);
     rd0.sssp_w = 4;
+    rd0.dp_wmax = std::min(32u, std::max(1u, env_u32("GSTB_DP_WMAX", 32)));
     CK(cudaMemcpy(d_rd, &rd0, sizeof(RoundDesc), cudaMemcpyHostToDevice));
   }
   // member items v*8 + j, staged through a fixed host array (calls are

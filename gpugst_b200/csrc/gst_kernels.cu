@@ -473,7 +473,7 @@ __device__ void dp_expand(const QDev& q, const GraphDev& g, uint32_t s, uint32_t
     const uint32_t lim = best - c;
     const uint32_t a0 = __ldg(g.beg + v);
     uint32_t a1 = arcs_upto(g, v, __ldg(g.beg + v + 1), lim);
-    if (rd->hub_on && a1 - a0 >= rd->hub_min_deg &&
+    if (rd->grow_chunks && a1 - a0 >= rd->hub_min_deg &&
         push_grow_chunks(rd, slot, false, s, a0 + GROW_LOCAL, a1, lane))
       a1 = a0 + GROW_LOCAL;
     grow_arcs(q, g, lane, v, p, comp, c, best, lim, -1, a0, a1, gc, wb);
@@ -568,7 +568,7 @@ __device__ void hop_expand(const QDev& q, const GraphDev& g, uint32_t s, uint32_
     const uint32_t lim = best - c;
     const uint32_t a0 = __ldg(g.beg + v);
     uint32_t a1 = arcs_upto(g, v, __ldg(g.beg + v + 1), lim);
-    if (rd->hub_on && a1 - a0 >= rd->hub_min_deg &&
+    if (rd->grow_chunks && a1 - a0 >= rd->hub_min_deg &&
         push_grow_chunks(rd, slot, true, s, a0 + GROW_LOCAL, a1, lane))
       a1 = a0 + GROW_LOCAL;
     grow_arcs(q, g, lane, v, p, comp, c, best, lim, (int)d + 1, a0, a1, gc, wb);
@@ -729,13 +729,7 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
   const uint32_t f1 = __shfl_sync(FULL, x, i1 - 1u);
   const uint32_t thi = q.theta_hi, nsh = near_sh(q.par ^ 1u);
   uint32_t* __restrict__ dist = q.dist_nx;  // targets: the rows this round writes
-  // Exact (Jacobi) rounds compare against the target's row of the previous
-  // round: the value the round must beat.  The written row can still hold
-  // the value of two rounds ago for a vertex that changed last round and has
-  // not copied its new value across yet; a comparison with it would write
-  // and flag non-improvements.
-  const bool jac = q.dist_nx != q.dist;
-  const uint32_t* __restrict__ prev = jac ? q.dist : q.dist_nx;
+
   for (uint32_t base = f0; base < f1; base += 32u * SSSP_U) {
     uint2 arc[SSSP_U];
     uint32_t itm[SSSP_U];
@@ -763,7 +757,7 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
     for (int u = 0; u < SSSP_U; u++) {
       ok[u] = ok[u] && arc[u].y <= h[itm[u]].lim;
       if (ok[u]) {
-        const uint4* row = reinterpret_cast<const uint4*>(prev + (size_t)arc[u].x * 8);
+        const uint4* row = reinterpret_cast<const uint4*>(dist + (size_t)arc[u].x * 8);
         ra[u] = __ldcg(row);
         rb[u] = __ldcg(row + 1);
       } else {
@@ -809,14 +803,12 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
 #pragma unroll
     for (int u = 0; u < SSSP_U; u++) {
       const uint32_t bits = (nn[u] << nsh) | (nf[u] << FAR_SH);
-      uint32_t fw = rb[u].w;
-      if (jac) {
-        // the row read was the previous round's: the flags of the written
-        // row come back from the OR itself
-        fw = bits ? atomicOr(dist + (size_t)arc[u].x * ROW + FLAGW, bits) : bits;
-      } else if (bits & ~fw) {
-        red_or(dist + (size_t)arc[u].x * ROW + FLAGW, bits);
-      }
+      // (exact rounds compare with the written row, the running minimum of
+      // the round: it filters repeated relaxations of a target far better
+      // than the previous round's row, at the price of a few entries for
+      // vertices whose own new value has not been carried across yet)
+      const uint32_t fw = rb[u].w;
+      if (bits & ~fw) red_or(dist + (size_t)arc[u].x * ROW + FLAGW, bits);
       tN[u] = nn[u] && ((fw >> nsh) & 0xFFu) == 0u;
       tF[u] = nf[u] && ((fw >> FAR_SH) & 0xFFu) == 0u;
       itv[u] = arc[u].x;
@@ -1189,8 +1181,38 @@ __device__ void tour_warp(const QDev& q, uint32_t lane) {
 // reads are one broadcast per warp; each lane packs 8 entries of its row
 // into one 16-byte store.  Items of different
 // queries in one task are handled run by run.
+// lower_bound_comp for a subset X that every lane of the warp evaluates at
+// the same time: the loops run over the groups of X only, and lane `lane`'s
+// capped distances are read from shared memory (sdl[j][lane]), where a
+// group index that varies inside the loop costs no local memory.
+__device__ __forceinline__ uint32_t lower_bound_uniform(const uint32_t (*sdl)[32], uint32_t lane, int k, uint32_t X,
+                                                        const uint32_t* __restrict__ P,
+                                                        const uint32_t* __restrict__ T2) {
+  const uint32_t K2 = 1u << k;
+  uint32_t lb0 = 0, mind = BIG;
+  for (uint32_t m = X; m; m &= m - 1u) {
+    const uint32_t d = sdl[__ffs(m) - 1][lane];
+    lb0 = max(lb0, d);
+    mind = min(mind, d);
+  }
+  uint32_t lb1 = BIG, lb2 = 0;
+  for (uint32_t mi = X; mi; mi &= mi - 1u) {
+    const uint32_t i = __ffs(mi) - 1;
+    const uint32_t di = sdl[i][lane];
+    const uint32_t* Pi = P + ((size_t)i * K2 + X) * k;
+    for (uint32_t mj = X; mj; mj &= mj - 1u) {
+      const uint32_t j = __ffs(mj) - 1;
+      const uint32_t t = sat_add(sat_add(di, __ldg(Pi + j)), sdl[j][lane]);
+      lb1 = min(lb1, (t + 1) >> 1);
+    }
+    const uint32_t t2 = sat_add(sat_add(di, __ldg(T2 + (size_t)i * K2 + X)), mind);
+    lb2 = max(lb2, (t2 + 1) >> 1);
+  }
+  return max(lb0, max(lb1 >= BIG ? BIG : lb1, lb2));
+}
+
 __device__ void lbt_rows32(const QDev* __restrict__ qd, const uint32_t* __restrict__ pre, int nslots, uint32_t n_lb,
-                           uint32_t task, uint32_t lane) {
+                           uint32_t task, uint32_t lane, uint32_t (*sdl)[32]) {
   const unsigned FULL = 0xFFFFFFFFu;
   const uint32_t it = task * 32u + lane;
   const bool valid = it < n_lb;
@@ -1208,7 +1230,6 @@ __device__ void lbt_rows32(const QDev* __restrict__ qd, const uint32_t* __restri
     const uint32_t* P = q.tour;
     const uint32_t* T2 = q.tour + (size_t)k * K2 * k;
     const uint32_t v = mine ? q.lb_off + (it - pre[si]) : 0u;
-    uint32_t dl[KMAX];
     {
       uint4 a = make_uint4(0u, 0u, 0u, 0u), b = a;
       if (mine) {
@@ -1218,8 +1239,9 @@ __device__ void lbt_rows32(const QDev* __restrict__ qd, const uint32_t* __restri
       }
       const uint32_t r[KMAX] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z};
 #pragma unroll
-      for (int j = 0; j < KMAX; j++) dl[j] = min(r[j], q.cap1);
+      for (int j = 0; j < KMAX; j++) sdl[j][lane] = min(r[j], q.cap1);
     }
+    __syncwarp();
     unsigned short* out = q.lbt + ((size_t)v << k);
     for (uint32_t x0 = 0; x0 < K2; x0 += 8u) {
       uint32_t pk[4];
@@ -1230,7 +1252,7 @@ __device__ void lbt_rows32(const QDev* __restrict__ qd, const uint32_t* __restri
         for (int e = 0; e < 2; e++) {
           const uint32_t X = x0 + 2u * h + e;
           uint32_t lb = 0;
-          if (X != 0u && X < K2) lb = lower_bound_comp(dl, k, X, P, T2);
+          if (X != 0u && X < K2) lb = lower_bound_uniform(sdl, lane, k, X, P, T2);
           const uint32_t ent = lb >= BIG ? LB_INF : min(lb, LB_INF - 1u);
           two |= ent << (16 * e);
         }
@@ -1244,37 +1266,53 @@ __device__ void lbt_rows32(const QDev* __restrict__ qd, const uint32_t* __restri
         }
       }
     }
+    __syncwarp();  // the next run reuses the distance stage
   }
 }
 
-// Weight of arc (a -> b): linear scan of a's weight-sorted adjacency.
-__device__ uint32_t arc_weight(const GraphDev& g, uint32_t a, uint32_t b) {
-  for (uint32_t x = g.beg[a]; x < g.beg[a + 1]; x++) {
-    uint2 arc = g.adj[x];
-    if (arc.x == b) return arc.y;
+// Weight of arc (a -> b): the warp scans a's weight-sorted adjacency, 32
+// arcs per step (hub lists hold tens of thousands of arcs).  Every lane calls
+// it with the same a and b.
+__device__ uint32_t arc_weight_warp(const GraphDev& g, uint32_t a, uint32_t b, uint32_t lane) {
+  const uint32_t x0 = __ldg(g.beg + a), x1 = __ldg(g.beg + a + 1);
+  for (uint32_t base = x0; base < x1; base += 32u) {
+    const uint32_t x = base + lane;
+    uint32_t w = INF32;
+    if (x < x1) {
+      const uint2 arc = __ldg(g.adj + x);
+      if (arc.x == b) w = arc.y;
+    }
+    const unsigned hit = __ballot_sync(0xFFFFFFFFu, w != INF32);
+    if (hit) return __shfl_sync(0xFFFFFFFFu, w, __ffs(hit) - 1);
   }
   return INF32;
 }
 
 // Follow parent words from the best full state, emitting (u, v, w) edges;
-// qbuf[0] serves as the explicit stack.  Run by one thread.
-__device__ void extract_one(const QDev& q, const GraphDev& g) {
+// qbuf[0] serves as the explicit stack.  Run by one warp: every lane walks
+// the same states (lane 0 alone writes), and the arc weights are looked up
+// by the whole warp.
+__device__ void extract_warp(const QDev& q, const GraphDev& g, uint32_t lane) {
   QCtl* ctl = q.ctl;
-  unsigned long long bf = ctl->best_full;
+  const unsigned long long bf = __ldcg(&ctl->best_full);
   if (bf == INF64) {
-    ctl->status = 1;
-    ctl->n_edges = 0;
+    if (lane == 0) {
+      ctl->status = 1;
+      ctl->n_edges = 0;
+    }
     return;
   }
   const int k = q.k, nd = q.nd;
   const bool hop = q.phase == PH_HOP;
-  uint32_t payload = (uint32_t)bf;
-  uint32_t root = hop ? payload >> 3 : payload;
-  uint32_t rd = hop ? (payload & 7u) : 0u;
+  const uint32_t payload = (uint32_t)bf;
+  const uint32_t root = hop ? payload >> 3 : payload;
+  const uint32_t rd = hop ? (payload & 7u) : 0u;
   uint32_t* stack = q.qbuf[0];
   uint32_t sp = 0;
-  uint32_t full = (uint32_t)q.full;
-  stack[sp++] = hop ? ((root << k) | full) * (uint32_t)nd + rd : ((root << k) | full);
+  const uint32_t full = (uint32_t)q.full;
+  if (lane == 0) stack[0] = hop ? ((root << k) | full) * (uint32_t)nd + rd : ((root << k) | full);
+  sp = 1;
+  __syncwarp();
   uint32_t ne = 0, steps = 0, status = 0;
   const uint32_t max_steps = 4u * g.V + 64u;
   while (sp > 0) {
@@ -1282,56 +1320,61 @@ __device__ void extract_one(const QDev& q, const GraphDev& g) {
       status = 2;
       break;
     }
-    uint32_t s = stack[--sp];
-    uint32_t d = hop ? s % (uint32_t)nd : 0u;
-    uint32_t vp = hop ? s / (uint32_t)nd : s;
-    uint32_t v = vp >> k, p = vp & ((1u << k) - 1u);
-    unsigned long long e = q.table[s];
+    const uint32_t s = __ldcg(stack + --sp);
+    __syncwarp();  // every lane has read the top before lane 0 overwrites it
+    const uint32_t d = hop ? s % (uint32_t)nd : 0u;
+    const uint32_t vp = hop ? s / (uint32_t)nd : s;
+    const uint32_t v = vp >> k, p = vp & ((1u << k) - 1u);
+    const unsigned long long e = __ldcg(q.table + s);
     if ((uint32_t)(e >> 32) == INF32) {
       status = 2;
       break;
     }
-    uint32_t par = (uint32_t)e;
-    uint32_t type = par >> 30;
+    const uint32_t par = (uint32_t)e;
+    const uint32_t type = par >> 30;
     if (type == 1u) {
-      uint32_t u = par & 0x3FFFFFFFu;
-      if (ne < q.max_edges) {
+      const uint32_t u = par & 0x3FFFFFFFu;
+      const uint32_t w = arc_weight_warp(g, v, u, lane);
+      if (lane == 0 && ne < q.max_edges) {
         q.out_edges[3 * ne] = u;
         q.out_edges[3 * ne + 1] = v;
-        q.out_edges[3 * ne + 2] = arc_weight(g, v, u);
+        q.out_edges[3 * ne + 2] = w;
       }
       ne++;
-      if (hop) {
-        if (d == 0) {
-          status = 2;
-          break;
-        }
-        stack[sp++] = ((u << k) | p) * (uint32_t)nd + d - 1;
-      } else {
-        stack[sp++] = (u << k) | p;
+      if (hop && d == 0) {
+        status = 2;
+        break;
       }
+      if (lane == 0) stack[sp] = hop ? ((u << k) | p) * (uint32_t)nd + d - 1 : ((u << k) | p);
+      sp++;
     } else if (type == 2u) {
-      uint32_t p1 = par & 0xFFu, p2 = p ^ p1;
+      const uint32_t p1 = par & 0xFFu, p2 = p ^ p1;
       if (p1 == 0 || p2 == 0 || (p1 & ~p) != 0) {
         status = 2;
         break;
       }
-      if (hop) {
-        uint32_t d1 = (par >> 8) & 7u, d2 = (par >> 11) & 7u;
-        stack[sp++] = ((v << k) | p1) * (uint32_t)nd + d1;
-        stack[sp++] = ((v << k) | p2) * (uint32_t)nd + d2;
-      } else {
-        stack[sp++] = (v << k) | p1;
-        stack[sp++] = (v << k) | p2;
+      if (lane == 0) {
+        if (hop) {
+          const uint32_t d1 = (par >> 8) & 7u, d2 = (par >> 11) & 7u;
+          stack[sp] = ((v << k) | p1) * (uint32_t)nd + d1;
+          stack[sp + 1] = ((v << k) | p2) * (uint32_t)nd + d2;
+        } else {
+          stack[sp] = (v << k) | p1;
+          stack[sp + 1] = (v << k) | p2;
+        }
       }
+      sp += 2;
     } else if (type != 0u) {
       status = 2;
       break;
     }
+    __syncwarp();  // lane 0's pushes are visible to the next pop
   }
-  ctl->status = status;
-  ctl->n_edges = ne;
-  ctl->root = root;
+  if (lane == 0) {
+    ctl->status = status;
+    ctl->n_edges = ne;
+    ctl->root = root;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1611,7 +1654,7 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
     uint32_t wd = 1;
     const unsigned long long n_dp = (unsigned long long)wsum[(blockDim.x >> 5) - 1][T_DP] +
                                     wsum[(blockDim.x >> 5) - 1][T_HOP];
-    while (wd < 32u && n_dp > 2ull * wd * rd->light_warps) wd <<= 1;
+    while (wd < rd->dp_wmax && n_dp > 2ull * wd * rd->light_warps) wd <<= 1;
     rd->dp_w = wd;
     const uint32_t per_task[NT] = {32, 32, 32, 1, 1, w, wd, wd, 32, 32};
     uint32_t off = 0;
@@ -1635,6 +1678,10 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
     // hub chunking pays off only when the round is too small to fill the GPU
     rd->hub_on =
         (rd->big != nullptr && rd->items[T_SSSP] + rd->items[T_DP] + rd->items[T_HOP] < rd->hub_max_items) ? 1u : 0u;
+    // DP tasks that hold several states hand their hub grows out in every
+    // round: a task with a few hub states would otherwise grow them one
+    // after another on one warp
+    rd->grow_chunks = (rd->big != nullptr && (rd->hub_on || wd > 1u)) ? 1u : 0u;
   }
 }
 
@@ -1687,7 +1734,7 @@ __global__ void __launch_bounds__(256, GSTB_LIGHT_MIN_BLOCKS) k_light(const QDev
     } else if (t == T_TOUR) {
       tour_warp(qd[find_slot(P, nslots, local)], lane);
     } else if (t == T_EXTRACT) {
-      if (lane == 0) extract_one(qd[find_slot(P, nslots, local)], g);
+      extract_warp(qd[find_slot(P, nslots, local)], g, lane);
     } else {
       const uint32_t it = local * 32u + lane;
       bool toN = false, toF = false;
@@ -1728,6 +1775,7 @@ __global__ void __launch_bounds__(256, 3) k_heavy(const QDev* __restrict__ qd, R
   nslots = min(nslots, (int)__ldcg(&rd->nslots));
   __shared__ uint32_t s_lb[MAX_SLOTS + 1];
   __shared__ RelaxHdr s_hub[8];
+  __shared__ uint32_t s_dl[8][KMAX][32];  // bound rows: each lane's capped distances
   __shared__ WarpStat s_ws[8];
   __shared__ WarpBuf s_wb[8];
   WarpStat& ws = s_ws[threadIdx.x >> 5];
@@ -1755,7 +1803,7 @@ __global__ void __launch_bounds__(256, 3) k_heavy(const QDev* __restrict__ qd, R
     }
     const uint32_t ht = task - nbig;
     if (ht < snap0) {  // lower-bound table rows, one vertex per lane
-      lbt_rows32(qd, s_lb, nslots, n_lb, ht, lane);
+      lbt_rows32(qd, s_lb, nslots, n_lb, ht, lane, s_dl[threadIdx.x >> 5]);
       continue;
     }
     // snapshot of a hop-bounded query's distance rows, one row per lane
