@@ -426,6 +426,9 @@ def main():
     ap.add_argument("--c5-max-pending", type=int, default=256)
     ap.add_argument("--c5-drain", type=float, default=5.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--c2-sweep", type=int, default=1,
+                    help="with the batched configuration, also run the plain path and the serving sweep on the "
+                         "170k-vertex workload (0: off)")
     args = ap.parse_args()
     big = args.workload in ("c4", "c4s")
     B = args.batch or (128 if big else 90)
@@ -563,6 +566,33 @@ def main():
             c5.append(open_loop(engine, E, c5reqs, rate, args.c5_seconds, seed=5000 + int(rate),
                                 max_pending=args.c5_max_pending, drain_s=args.c5_drain))
 
+    # the same trade-off on the 170k-vertex workload (smaller queries: a
+    # single one does not fill the GPU)
+    c2 = None
+    if big and args.c2_sweep and rank == 0:
+        E.close()
+        g2, gr2, qs2, Ds2 = load_workload("c2")
+        E = engine.Engine.from_instance(g2, gr2)
+        E.query_batch(qs2[:90], Ds2[:90])
+        pl = []
+        for i in range(100):
+            t0 = time.perf_counter()
+            E.query(qs2[i], D=Ds2[i])
+            pl.append(1e3 * (time.perf_counter() - t0))
+        p_qps = len(pl) / (sum(pl) / 1e3)
+        t0 = time.perf_counter()
+        rb = E.query_batch(qs2[100:190], Ds2[100:190])
+        b_qps = 90 / (time.perf_counter() - t0)
+        sw2 = []
+        reqs2 = [(qs2[(11 * i) % len(qs2)], Ds2[(11 * i) % len(qs2)]) for i in range(256)]
+        for inflight in [int(x) for x in args.sweep.split(",") if x]:
+            qps, lats, _ = closed_loop(engine, E, reqs2, inflight)
+            sw2.append({"inflight": inflight, "qps": qps, "p50_ms": pct(lats, 50), "p99_ms": pct(lats, 99),
+                        "vs_plain": qps / p_qps, "queries": len(reqs2)})
+        c2 = {"workload": workload_desc("c2"), "plain_qps": p_qps, "plain_p50_ms": pct(pl, 50),
+              "plain_p99_ms": pct(pl, 99), "batched_qps_e2e": b_qps, "batched_vs_plain_e2e": b_qps / p_qps,
+              "batched_device_ms": rb[0].device_ms, "serve_sweep": sw2}
+
     if rank == 0:
         best_pt = max(sweep, key=lambda x: x["qps"]) if sweep else None
         out = {
@@ -595,6 +625,7 @@ def main():
             "serve_sweep": sweep,
             "serve_vs_plain_best": best_pt["vs_plain"] if best_pt else None,
             "open_loop": c5,
+            "c2_170k": c2,
             "roofline": {"bound": "hbm", "kernel": "round (k_light + k_heavy)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": (per_round_alg * tpb) if tpb else None,
