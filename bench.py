@@ -291,7 +291,7 @@ def run_reference(args, g, gr, qs, Ds, rank, world):
     big = args.workload in ("c4", "c4s")
     try:
         import psutil
-        per_proc = (16 << 30) if big else (3 << 30)
+        per_proc = (6 << 30) if big else (3 << 30)  # peak RSS of one process: about 4 GB on the 3M-vertex graph
         mem_workers = int(psutil.virtual_memory().available / per_proc)
     except Exception:
         mem_workers = nproc

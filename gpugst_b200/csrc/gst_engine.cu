@@ -410,6 +410,13 @@ class Runner {
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bh, k_heavy, 256, 0));
       light_grid_ = (unsigned)g_->num_sms * (unsigned)std::max(1, bl);
       heavy_grid_ = (unsigned)g_->num_sms * (unsigned)std::max(1, bh);
+      resident_light_warps_ = light_grid_ * (256 / 32);
+      // GSTB_GRID_WAVES > 1 launches that many resident waves of blocks: a
+      // block that runs out of tasks early exits and a waiting block takes
+      // its place on the SM
+      const unsigned waves = std::min(8u, std::max(1u, env_u32("GSTB_GRID_WAVES", 1)));
+      light_grid_ *= waves;
+      heavy_grid_ *= waves;
     }
     {
       // hub arc chunk list (k_light -> k_heavy within a round)
@@ -422,7 +429,7 @@ class Runner {
       rd.hub_min_deg = g_->tune.hub_min_deg;
       rd.hub_min_rest = env_u32("GSTB_HUB_MIN_REST", 128);
       rd.hub_max_items = env_u32("GSTB_HUB_MAX_ITEMS", 1000000);
-      rd.light_warps = light_grid_ * (256 / 32);
+      rd.light_warps = resident_light_warps_;  // task widths are sized for the warps resident at once
       rd.sssp_w = 4;
       rd.dp_wmax = std::min(32u, std::max(1u, env_u32("GSTB_DP_WMAX", 32)));
       CK(cudaMemcpy(d_rd_, &rd, sizeof(rd), cudaMemcpyHostToDevice));
@@ -942,7 +949,7 @@ class Runner {
   uint32_t delta_sssp_ = 8, delta_dp_ = 2, max_edges_dev_ = 1u << 16;
   uint32_t cap_num_ = 1, cap_den_ = 2, rounds_per_sync_ = 6;
   cudaEvent_t ev_[2] = {};
-  unsigned light_grid_ = 148 * 4, heavy_grid_ = 148 * 2;
+  unsigned light_grid_ = 148 * 4, heavy_grid_ = 148 * 2, resident_light_warps_ = 148 * 4 * 8;
   double last_call_ms_ = 0;
   double trace_ms_ = 0;
   cudaGraphExec_t round_graph_ = nullptr;

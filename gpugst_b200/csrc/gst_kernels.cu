@@ -278,22 +278,31 @@ __device__ __forceinline__ void grow_arcs(const QDev& q, const GraphDev& g, uint
       ok[u] = a < a1;
       arc[u] = ok[u] ? __ldg(g.adj + a) : make_uint2(0u, 0u);
     }
-    uint32_t t[GROW_U], cur[GROW_U], lbu[GROW_U];
+    // the target's bound first: it rejects most targets (a neighbour of a
+    // hub is rarely close to the missing groups), and only the targets it
+    // passes need their 8-byte table word (another random sector)
+    uint32_t t[GROW_U], cur[GROW_U], lbu[GROW_U], nc[GROW_U];
+    bool want[GROW_U];
 #pragma unroll
     for (int u = 0; u < GROW_U; u++) {
       ok[u] = ok[u] && arc[u].y <= lim;
       const uint32_t vp = (arc[u].x << k) | p;
       t[u] = dnext < 0 ? vp : vp * nd + (uint32_t)dnext;
-      cur[u] = ok[u] ? (uint32_t)(ld_cg(q.table + t[u]) >> 32) : 0u;
       lbu[u] = ok[u] ? (uint32_t)__ldg(lbt + ((size_t)arc[u].x << k) + comp) : 0u;
     }
-    bool want[GROW_U];
-    uint32_t nc[GROW_U];
+    bool any = false;
 #pragma unroll
     for (int u = 0; u < GROW_U; u++) {
       nc[u] = c + arc[u].y;
-      want[u] = ok[u] && nc[u] < cur[u] && lb_ok(nc[u], lbu[u], best);
+      want[u] = ok[u] && lb_ok(nc[u], lbu[u], best);
+      any = any || want[u];
       if (ok[u]) cnt.arcs++;
+    }
+    if (__any_sync(0xFFFFFFFFu, any)) {
+#pragma unroll
+      for (int u = 0; u < GROW_U; u++) cur[u] = want[u] ? (uint32_t)(ld_cg(q.table + t[u]) >> 32) : 0u;
+#pragma unroll
+      for (int u = 0; u < GROW_U; u++) want[u] = want[u] && nc[u] < cur[u];
     }
     if (dnext >= 0) {
       // hop-bounded target (u, p, dnext): its missing groups must stay within
@@ -1184,31 +1193,41 @@ __device__ void tour_warp(const QDev& q, uint32_t lane) {
 // lower_bound_comp for a subset X that every lane of the warp evaluates at
 // the same time: the loops run over the groups of X only, and lane `lane`'s
 // capped distances are read from shared memory (sdl[j][lane]), where a
-// group index that varies inside the loop costs no local memory.
+// group index that varies inside the loop costs no local memory.  Same value
+// as lower_bound_comp, with less work:
+//   - each unordered pair {i, j} is visited once with the cheaper of the two
+//     orders P[i][X][j], P[j][X][i] (the ordered pairs (i, j) and (j, i) give
+//     d_i + P[i][X][j] + d_j and d_j + P[j][X][i] + d_i); a pair (i, i) only
+//     exists for X = {i}, where every bound is d_i;
+//   - each term is a sum of three values <= 2^30, which cannot overflow 32
+//     bits, and saturation at BIG and the halving are monotone, so both are
+//     applied once to the minimum (lb1) or maximum (lb2) instead of per term.
 __device__ __forceinline__ uint32_t lower_bound_uniform(const uint32_t (*sdl)[32], uint32_t lane, int k, uint32_t X,
                                                         const uint32_t* __restrict__ P,
                                                         const uint32_t* __restrict__ T2) {
   const uint32_t K2 = 1u << k;
+  if ((X & (X - 1u)) == 0u) return sdl[__ffs(X) - 1][lane];  // a single group
   uint32_t lb0 = 0, mind = BIG;
   for (uint32_t m = X; m; m &= m - 1u) {
     const uint32_t d = sdl[__ffs(m) - 1][lane];
     lb0 = max(lb0, d);
     mind = min(mind, d);
   }
-  uint32_t lb1 = BIG, lb2 = 0;
+  uint32_t m1 = 0xFFFFFFFFu, m2 = 0;
   for (uint32_t mi = X; mi; mi &= mi - 1u) {
     const uint32_t i = __ffs(mi) - 1;
     const uint32_t di = sdl[i][lane];
     const uint32_t* Pi = P + ((size_t)i * K2 + X) * k;
-    for (uint32_t mj = X; mj; mj &= mj - 1u) {
+    for (uint32_t mj = mi & (mi - 1u); mj; mj &= mj - 1u) {  // the groups of X above i
       const uint32_t j = __ffs(mj) - 1;
-      const uint32_t t = sat_add(sat_add(di, __ldg(Pi + j)), sdl[j][lane]);
-      lb1 = min(lb1, (t + 1) >> 1);
+      const uint32_t pij = min(__ldg(Pi + j), __ldg(P + ((size_t)j * K2 + X) * k + i));
+      m1 = min(m1, di + pij + sdl[j][lane]);
     }
-    const uint32_t t2 = sat_add(sat_add(di, __ldg(T2 + (size_t)i * K2 + X)), mind);
-    lb2 = max(lb2, (t2 + 1) >> 1);
+    m2 = max(m2, di + __ldg(T2 + (size_t)i * K2 + X) + mind);
   }
-  return max(lb0, max(lb1 >= BIG ? BIG : lb1, lb2));
+  const uint32_t lb1 = (min(m1, BIG) + 1u) >> 1;
+  const uint32_t lb2 = (min(m2, BIG) + 1u) >> 1;
+  return max(lb0, max(lb1, lb2));
 }
 
 __device__ void lbt_rows32(const QDev* __restrict__ qd, const uint32_t* __restrict__ pre, int nslots, uint32_t n_lb,

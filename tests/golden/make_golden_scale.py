@@ -11,12 +11,20 @@ Writes golden_scale.json:
       compiled unchanged).  A query that does not finish within --limit
       seconds is left out and listed under "skipped".
 
+  c4  Chung-Lu V=3,000,000, E=117M (gen.config4, the batched configuration):
+      the first 8 unbounded k = 3 and 4 unbounded k = 4 queries of its
+      1,024-query set, solved by prunedpp_ref fed raw arrays (--bin: the
+      reference's own structures, without the minutes its text parser needs
+      at this size), and the first 6 hop-bounded queries with k <= 4, solved
+      by the HOP_cpu restatement (oracle.hop; the reference's HOP_cpu has no
+      raw-array driver).  Each entry records its source.
+
 Each instance is regenerated by the tests from its seeded spec; the
 fingerprint (SHA-256 over the CSR and group arrays) lets a test detect a
 generator that no longer reproduces the instance the costs belong to.
 
 Run where oracle/_ref has been built (make -C oracle ref):
-    python tests/golden/make_golden_scale.py [--limit 240] [--jobs 8]
+    python tests/golden/make_golden_scale.py [--limit 240] [--jobs 8] [--only c2,c3,c4]
 """
 import argparse
 import concurrent.futures as cf
@@ -58,6 +66,64 @@ def instance(name):
     return g, gr, sel, {f"k{k}_D{D}": D for k in (3, 4, 5) for D in (2, 3, 4)}
 
 
+def _hop_one(args):
+    """oracle.hop on one c4 query (run in a worker process)."""
+    i, q, D = args
+    from oracle import oracle
+    g, gr, _, _ = _C4
+    t0 = time.time()
+    r = oracle.hop(g, gr, q, D)
+    return i, r.status, r.cost, time.time() - t0
+
+
+_C4 = None
+
+
+def make_c4(gold, jobs, limit):
+    """The c4 entries (see the module docstring)."""
+    global _C4
+    import multiprocessing as mp
+    g, gr, qs, Ds = gen.config4()
+    _C4 = (g, gr, qs, Ds)
+    gold["fingerprint"]["c4"] = fingerprint(g, gr)
+    un3 = [i for i in range(len(qs)) if Ds[i] < 0 and len(qs[i]) == 3][:8]
+    un4 = [i for i in range(len(qs)) if Ds[i] < 0 and len(qs[i]) == 4][:4]
+    hop = [i for i in range(len(qs)) if Ds[i] >= 0 and len(qs[i]) <= 4][:6]
+    res = {"index": [], "queries": [], "D": [], "cost": [], "feasible": [], "seconds": [], "source": []}
+    with tempfile.TemporaryDirectory() as td:
+        pre = os.path.join(td, "c4")
+        g.beg_pos.astype(np.uint32).tofile(pre + ".beg")
+        g.csr.astype(np.uint32).tofile(pre + ".adj")
+        g.weight.astype(np.int32).tofile(pre + ".w")
+        gr.ptr.astype(np.uint64).tofile(pre + ".gptr")
+        gr.members.astype(np.uint32).tofile(pre + ".gv")
+        cmds = {}
+        for k, idx in ((3, un3), (4, un4)):
+            np.array([qs[i] for i in idx], dtype=np.uint32).tofile(f"{pre}.q{k}")
+            for r, i in enumerate(idx):
+                cmds[i] = [os.path.join(REF_BIN, "prunedpp_ref"), "--bin", pre, str(k), str(r), str(r), "0"]
+        with cf.ThreadPoolExecutor(jobs) as ex:
+            futs = {ex.submit(run_one, cmd, limit): i for i, cmd in cmds.items()}
+            for fu in cf.as_completed(futs):
+                i = futs[fu]
+                r, wall = fu.result()
+                print("c4", i, r, f"{wall:.0f} s", flush=True)
+                if r is None:
+                    continue
+                for key, val in (("index", i), ("queries", qs[i].tolist()), ("D", -1), ("cost", r["cost"]),
+                                 ("feasible", r["feasible"]), ("seconds", r["seconds"]),
+                                 ("source", "reference PrunedDP++ (prunedpp_ref --bin, exact mode)")):
+                    res[key].append(val)
+    with mp.get_context("fork").Pool(min(jobs, len(hop))) as pool:
+        for i, st, cost, sec in pool.imap_unordered(_hop_one, [(i, qs[i], Ds[i]) for i in hop]):
+            print("c4 hop", i, st, cost, f"{sec:.0f} s", flush=True)
+            for key, val in (("index", i), ("queries", qs[i].tolist()), ("D", Ds[i]), ("cost", cost if st == 0 else 0),
+                             ("feasible", 1 if st == 0 else 0), ("seconds", sec),
+                             ("source", "HOP_cpu restatement (oracle.hop)")):
+                res[key].append(val)
+    gold["results"]["c4"] = res
+
+
 def run_one(cmd, limit):
     t0 = time.time()
     try:
@@ -82,8 +148,12 @@ def main():
     if os.path.exists(path):
         with open(path) as f:
             gold = json.load(f)
+    names = args.only.split(",")
+    if "c4" in names:
+        make_c4(gold, args.jobs, args.limit)
+        names.remove("c4")
     with tempfile.TemporaryDirectory() as td:
-        for name in args.only.split(","):
+        for name in names:
             g, gr, sel, Ds = instance(name)
             gold["fingerprint"][name] = fingerprint(g, gr)
             # one query file per key: <name>_<key><k>.csv, read by the reference drivers

@@ -132,3 +132,28 @@ def test_k7_small_vs_oracle(gst_lib, oracle_mod):
                 bad.append((seed, D, "invalid tree"))
         E.close()
     assert not bad, bad
+
+
+def test_batched_configuration_matches_reference(gst_lib, oracle_mod):
+    """The 3M-vertex / 117M-edge batched configuration: unbounded queries
+    against the reference's own PrunedDP++ and hop-bounded ones against the
+    HOP_cpu restatement (golden_scale.json "c4"), through the batched and the
+    plain path, every tree validated."""
+    eng, O = gst_lib, oracle_mod
+    gold = _gold()
+    if "c4" not in gold["results"]:
+        pytest.skip("no c4 entries in golden_scale.json")
+    g, gr, _, _ = gen.config4()
+    assert _fingerprint(g, gr) == gold["fingerprint"]["c4"], "generator no longer reproduces the instance"
+    r = gold["results"]["c4"]
+    cases = [("c4", np.array(q, dtype=np.uint32), D, c if ok else None)
+             for q, D, c, ok in zip(r["queries"], r["D"], r["cost"], r["feasible"])]
+    assert len(cases) >= 12
+    E = eng.Engine.from_instance(g, gr)
+    try:
+        batch = E.query_batch([c[1] for c in cases], [c[2] for c in cases])
+        plain = [E.query(q, D=D) for _, q, D, _ in cases]
+    finally:
+        E.close()
+    bad = _check(eng, O, g, gr, cases, batch, "batch") + _check(eng, O, g, gr, cases, plain, "plain")
+    assert not bad, bad[:10]
