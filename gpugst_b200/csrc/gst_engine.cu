@@ -16,6 +16,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -36,6 +37,7 @@ namespace gstb {
 __global__ void k_control(QDev*, QCtl*, int, RoundDesc*, uint32_t*);
 __global__ void k_light(const QDev*, RoundDesc*, const uint32_t*, int, GraphDev);
 __global__ void k_heavy(const QDev*, RoundDesc*, const uint32_t*, int, GraphDev);
+__global__ void k_init_workspace(uint4*, size_t, uint4*, uint4*, uint32_t, uint4*, size_t);
 }  // namespace gstb
 
 using namespace gstb;
@@ -198,7 +200,15 @@ class Arena {
     n = align_up(std::max<size_t>(n, 1), 256);
     auto it = by_size_.lower_bound(n);
     if (it == by_size_.end()) {
-      if (!grow(n)) return nullptr;
+      // A growth of this size already failed and nothing has been freed
+      // since: waiting for running queries is cheaper than another failing
+      // cudaMalloc (and its trim) on every admission attempt, which stalled
+      // the host while the GPU ran out of launched rounds.
+      if (n >= grow_failed_) return nullptr;
+      if (!grow(n)) {
+        grow_failed_ = n;
+        return nullptr;
+      }
       it = by_size_.lower_bound(n);
       if (it == by_size_.end()) return nullptr;
     }
@@ -220,6 +230,7 @@ class Arena {
     size_t n = u->second;
     used_.erase(u);
     in_use_ -= n;
+    grow_failed_ = SIZE_MAX;  // a larger block may fit now
     const char* base = chunk_base(p);
     // merge with the free neighbours inside the same chunk
     auto nx = free_.find(p + n);
@@ -268,6 +279,7 @@ class Arena {
   // Give chunks that are entirely free back to the driver (a request larger
   // than every free block can then get one allocation of its own).
   void trim() {
+    grow_failed_ = SIZE_MAX;  // the device gets memory back
     for (auto it = chunks_.begin(); it != chunks_.end();) {
       auto f = free_.find(it->first);
       if (f != free_.end() && f->second == it->second) {
@@ -291,7 +303,10 @@ class Arena {
       sz = n;
       if (cudaMalloc(&p, sz) != cudaSuccess) {
         cudaGetLastError();
-        trim();  // free chunks may be what the device is missing
+        // free chunks may be what the device is missing; give them back only
+        // when no workspace is in use (cudaFree synchronises the device)
+        if (in_use_ != 0) return false;
+        trim();
         if (cudaMalloc(&p, sz) != cudaSuccess) {
           cudaGetLastError();
           return false;
@@ -331,6 +346,7 @@ class Arena {
   std::multimap<size_t, char*> by_size_;  // size -> free block
   std::unordered_map<char*, size_t> used_;
   size_t held_ = 0, in_use_ = 0, free_total_ = 0;
+  size_t grow_failed_ = SIZE_MAX;  // smallest growth that failed since the last free
   std::atomic<int>* fail_ = nullptr;
 };
 
@@ -611,15 +627,14 @@ class Runner {
     memset(&j->ctl, 0, sizeof(j->ctl));
     j->ctl.best = INF32;
     j->ctl.best_full = INF64;
-    cudaMemsetAsync(q.table, 0xFF, (size_t)g_->V * j->WT * 8, stream_);
-    // distances unknown, no group pending (word FLAGW of every row)
-    cudaMemsetAsync(q.dist, 0xFF, (size_t)g_->V * ROW * 4, stream_);
-    cudaMemset2DAsync(q.dist + FLAGW, ROW * 4, 0, 4, g_->V, stream_);
-    if (q.dist_nx != q.dist) {
-      cudaMemsetAsync(q.dist_nx, 0xFF, (size_t)g_->V * ROW * 4, stream_);
-      cudaMemset2DAsync(q.dist_nx + FLAGW, ROW * 4, 0, 4, g_->V, stream_);
-    }
-    cudaMemsetAsync(q.dflag, 0, L.qbuf - L.dflag, stream_);
+    // state table INF, distances unknown with no group pending, no state
+    // flag set: one launch (the byte counts are multiples of 16: the table
+    // holds an even number of 8-byte words, the flags span is 256-aligned)
+    k_init_workspace<<<(unsigned)g_->num_sms * 8u, 256, 0, stream_>>>(
+        reinterpret_cast<uint4*>(q.table), (size_t)g_->V * j->WT * 8 / 16, reinterpret_cast<uint4*>(q.dist),
+        q.dist_nx != q.dist ? reinterpret_cast<uint4*>(q.dist_nx) : nullptr, g_->V,
+        reinterpret_cast<uint4*>(q.dflag), (L.qbuf - L.dflag) / 16);
+    g_->launches++;
     // stage the member list and both descriptors in pinned memory; it is not
     // reused before the stream synchronises at the end of the next round block
     char* st = h_stage_ + (size_t)sh * (stage_cap_ / 2) + stage_off_[sh];

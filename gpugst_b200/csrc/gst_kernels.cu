@@ -1397,6 +1397,32 @@ __device__ void extract_warp(const QDev& q, const GraphDev& g, uint32_t lane) {
 }
 
 // ---------------------------------------------------------------------------
+// Workspace initialisation of an admitted query, one launch: the state table
+// to INF (all ones), both distance-row buffers to "unknown" (words 0..6 all
+// ones) with no group pending (word 7 zero), and the state flags to zero.
+// 16-byte stores, grid-stride.  (Replaces several memsets per query, one of
+// them a 2D memset over V rows of 4 bytes.)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_init_workspace(uint4* __restrict__ table, size_t table_vec,
+                                                        uint4* __restrict__ dist, uint4* __restrict__ dist2,
+                                                        uint32_t nv, uint4* __restrict__ dflag, size_t dflag_vec) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint4 ones = make_uint4(INF32, INF32, INF32, INF32);
+  const uint4 tail = make_uint4(INF32, INF32, INF32, 0u);
+  for (size_t i = tid; i < table_vec; i += stride) table[i] = ones;
+  for (size_t v = tid; v < nv; v += stride) {
+    dist[2 * v] = ones;
+    dist[2 * v + 1] = tail;
+    if (dist2 != nullptr) {
+      dist2[2 * v] = ones;
+      dist2[2 * v + 1] = tail;
+    }
+  }
+  for (size_t i = tid; i < dflag_vec; i += stride) dflag[i] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// ---------------------------------------------------------------------------
 // Control: one thread per slot.  Absorbs the previous round's counters,
 // decides this round's action, and publishes per-type item counts as
 // exclusive prefix sums over slots (pre[t][0..nslots]).
