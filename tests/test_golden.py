@@ -84,3 +84,28 @@ def test_oracle_matches_reference_at_scale(oracle_mod):
                 elif o.status != 0 or o.cost != c:
                     bad.append((name, key, q.tolist(), c, o.cost))
     assert n >= 12 and not bad, bad
+
+
+def test_batched_configuration_fixture(oracle_mod):
+    """The 3M-vertex batched configuration: the seeded generator reproduces
+    the fingerprinted instance, and the restatement agrees with the
+    reference's PrunedDP++ on the fixture's quickest unbounded query."""
+    import hashlib
+    import json
+    import os
+
+    from gpugst_b200 import gen
+    with open(os.path.join(golden_util.HERE, "golden_scale.json")) as f:
+        gold = json.load(f)
+    r = gold["results"]["c4"]
+    g, gr, qs, Ds = gen.config4()
+    h = hashlib.sha256()
+    for a in (g.beg_pos, g.csr, g.weight, gr.ptr, gr.members):
+        h.update(np.ascontiguousarray(a).tobytes())
+    assert h.hexdigest() == gold["fingerprint"]["c4"]
+    cand = [i for i, (D, src) in enumerate(zip(r["D"], r["source"])) if D < 0 and src.startswith("reference")]
+    i = min(cand, key=lambda x: r["seconds"][x])
+    q = np.array(r["queries"][i], dtype=np.uint32)
+    assert (q == qs[r["index"][i]]).all()
+    o = oracle_mod.prunedpp(g, gr, q, 0)
+    assert o.status == 0 and o.cost == r["cost"][i]
