@@ -69,11 +69,26 @@ struct RoundDesc {
   uint32_t sssp_w;        // distance items per warp task this round (set by k_control)
   uint32_t dp_w;          // DP states per warp task this round (set by k_control)
   uint32_t dp_wmax;       // largest DP task width (set by the host)
+  uint32_t sssp_wmax;     // largest distance task width, at most SSSP_WMAX (set by the host)
+  uint32_t merge_stage;   // a DP state with at least this many merge partners stages its row (0: never; host)
   uint32_t light_warps;   // warps of one k_light launch (set by the host)
   uint32_t nslots;        // 1 + the highest slot in use this round (set by k_control)
   // work stealing: a warp that finished its first task takes the next one
   // from these counters (zeroed by k_control every round)
   uint32_t next_light, next_heavy;
+};
+// State of one persistent round launch (k_rounds), written by the host
+// before each launch (the counters zero).
+struct PersistCtl {
+  uint32_t epoch;    // control steps published (round r's work waits for epoch >= r + 1)
+  uint32_t arrive;   // blocks that finished their round work, summed over rounds
+  uint32_t phase1;   // blocks that finished the light and static heavy tasks, summed over rounds
+  uint32_t err;      // 1: a bounded wait expired, the launch stopped
+  uint32_t err_where;  // the first wait that expired: 1 control step, 2 light tasks
+  uint32_t rounds;   // rounds completed
+  uint32_t hold;     // 1: control steps are not published (makes the waits expire; a test of them)
+  uint32_t pad;
+  unsigned long long timeout_ns;  // limit of every wait
 };
 constexpr uint32_t HUB_CHUNK = 256;     // arcs per chunk (one warp)
 constexpr uint32_t LB_CHUNK = 1u << 22; // bound-table rows (vertices) per query per round
@@ -217,6 +232,14 @@ __device__ __forceinline__ void red_or(uint32_t* p, uint32_t v) {
   asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Loads of data that a launch may itself have written in an earlier round
+// (distance rows, bound and tour tables): cached in L1, but as ordinary weak
+// loads, which the fences between rounds order.  The non-coherent read-only
+// path (__ldg) is kept for data that no launch writes (the graph, member lists).
+template <class T>
+__device__ __forceinline__ T ld_round(const T* p) {
+  return __ldca(p);
+}
 __device__ __forceinline__ uint32_t ld_cg(const uint32_t* p) { return __ldcg(p); }
 // The incumbent through L1: a value cached earlier in the same launch can be
 // higher than the current one, which only weakens pruning (every use of best
@@ -268,10 +291,10 @@ __device__ __forceinline__ uint32_t lower_bound_comp(const uint32_t (&dl)[KMAX],
 #pragma unroll
       for (int j = 0; j < KMAX; j++)
         if (j < k && (comp >> j & 1u)) {
-          uint32_t t = sat_add(sat_add(dl[i], __ldg(Pi + j)), dl[j]);
+          uint32_t t = sat_add(sat_add(dl[i], ld_round(Pi + j)), dl[j]);
           lb1 = min(lb1, (t + 1) >> 1);
         }
-      uint32_t t2 = sat_add(sat_add(dl[i], __ldg(T2 + (size_t)i * K2 + comp)), mind);
+      uint32_t t2 = sat_add(sat_add(dl[i], ld_round(T2 + (size_t)i * K2 + comp)), mind);
       lb2 = max(lb2, (t2 + 1) >> 1);
     }
   }

@@ -38,6 +38,7 @@ __global__ void k_control(QDev*, QCtl*, int, RoundDesc*, uint32_t*);
 __global__ void k_light(const QDev*, RoundDesc*, const uint32_t*, int, GraphDev);
 __global__ void k_heavy(const QDev*, RoundDesc*, const uint32_t*, int, GraphDev);
 __global__ void k_init_workspace(uint4*, size_t, uint4*, uint4*, uint32_t, uint4*, size_t);
+__global__ void k_rounds(QDev*, QCtl*, int, RoundDesc*, uint32_t*, GraphDev, uint32_t, PersistCtl*);
 }  // namespace gstb
 
 using namespace gstb;
@@ -82,7 +83,10 @@ struct gst_graph {
   std::atomic<uint64_t> launches{0};
   // fault injection (gst_debug_fail_allocs): workspace allocations still to fail
   std::atomic<int> fail_allocs{0};
+  // test hook of the persistent launch (gst_debug_hold_rounds)
+  std::atomic<uint32_t> hold_rounds{0}, wait_ms{0};
   bool profile = false;
+  bool prof_persistent = false;  // the profiled rounds ran as persistent launches
   double prof_light_ms = 0, prof_heavy_ms = 0;
   uint64_t prof_rounds = 0;
   uint64_t prof_stats[GST_NSTATS] = {0};
@@ -94,6 +98,8 @@ bool has_groups(gst_graph* g) {
   std::shared_lock<std::shared_mutex> lock(g->grp_mu);
   return !g->grp_ptr.empty();
 }
+
+uint32_t floor_pow2(uint32_t x) { return x ? 1u << (31 - __builtin_clz(x)) : 0u; }
 
 uint32_t env_u32(const char* name, uint32_t def) {
   const char* s = getenv(name);
@@ -413,8 +419,9 @@ class Runner {
     cap_num_ = g_->tune.cap_pct;
     cap_den_ = 100;
     max_edges_dev_ = env_u32("GSTB_MAX_TREE_EDGES", 1u << 16);
-    rounds_per_sync_ = std::min(64u, std::max(1u, env_u32("GSTB_ROUNDS_PER_SYNC", 4)));
+    rounds_per_sync_ = g_->tune.rounds_per_launch;
     trace_ms_ = (double)env_u32("GSTB_TRACE_MS", 0);  // report host iterations slower than this
+    wait_ms_default_ = std::max(1u, env_u32("GSTB_WAIT_MS", 30000));  // limit of a persistent launch's waits
     max_slots_ = std::min<uint32_t>(MAX_SLOTS - 1, std::max(1u, env_u32("GSTB_MAX_SLOTS", MAX_SLOTS - 1)));
     CK(cudaMalloc(&d_qd_, MAX_SLOTS * sizeof(QDev)));
     CK(cudaMalloc(&d_ctl_, MAX_SLOTS * sizeof(QCtl)));
@@ -433,6 +440,12 @@ class Runner {
       const unsigned waves = std::min(8u, std::max(1u, env_u32("GSTB_GRID_WAVES", 1)));
       light_grid_ *= waves;
       heavy_grid_ *= waves;
+      // the persistent round launch: one resident wave, every block at once
+      int br = 0, coop = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&br, k_rounds, 256, 0));
+      CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, g_->device));
+      rounds_grid_ = coop ? (unsigned)g_->num_sms * (unsigned)std::max(0, br) : 0u;
+      persist_ = rounds_grid_ > 0 && g_->tune.persistent;
     }
     {
       // hub arc chunk list (k_light -> k_heavy within a round)
@@ -445,9 +458,12 @@ class Runner {
       rd.hub_min_deg = g_->tune.hub_min_deg;
       rd.hub_min_rest = env_u32("GSTB_HUB_MIN_REST", 128);
       rd.hub_max_items = env_u32("GSTB_HUB_MAX_ITEMS", 1000000);
-      rd.light_warps = resident_light_warps_;  // task widths are sized for the warps resident at once
+      // task widths are sized for the warps resident at once
+      rd.light_warps = persist_ ? rounds_grid_ * (256 / 32) : resident_light_warps_;
       rd.sssp_w = 4;
-      rd.dp_wmax = std::min(32u, std::max(1u, env_u32("GSTB_DP_WMAX", 32)));
+      rd.dp_wmax = g_->tune.dp_wmax;
+      rd.sssp_wmax = g_->tune.sssp_wmax;
+      rd.merge_stage = g_->tune.merge_stage;
       CK(cudaMemcpy(d_rd_, &rd, sizeof(rd), cudaMemcpyHostToDevice));
     }
     CK(cudaMalloc(&d_pre_, (size_t)NT * (MAX_SLOTS + 1) * 4));
@@ -457,6 +473,9 @@ class Runner {
     CK(cudaMallocHost(&h_rd_, sizeof(RoundDesc)));
     CK(cudaMallocHost(&h_qd_, sizeof(QDev)));
     CK(cudaMallocHost(&h_one_, sizeof(uint32_t)));
+    CK(cudaMalloc(&d_pc_, sizeof(PersistCtl)));
+    CK(cudaMallocHost(&h_pc_, 4 * sizeof(PersistCtl)));  // launch templates, then read-backs, per block half
+    memset(h_pc_, 0, 4 * sizeof(PersistCtl));
     if (env_u32("GSTB_TRACE_ROUNDS", 0)) CK(cudaMallocHost(&h_rdtrace_, 2 * 64 * sizeof(RoundDesc)));
     *h_one_ = 1u;
     // pinned staging for admissions (descriptors + member lists) and for the
@@ -489,6 +508,10 @@ class Runner {
     if (h_rd_) cudaFreeHost(h_rd_);
     if (h_qd_) cudaFreeHost(h_qd_);
     if (h_one_) cudaFreeHost(h_one_);
+    if (h_pc_) cudaFreeHost(h_pc_);
+    h_pc_ = nullptr;
+    if (d_pc_) cudaFree(d_pc_);
+    d_pc_ = nullptr;
     if (h_rdtrace_) cudaFreeHost(h_rdtrace_);
     h_rdtrace_ = nullptr;
     h_one_ = nullptr;
@@ -559,9 +582,25 @@ class Runner {
     delta_dp_ = g_->tune.delta_dp;
     cap_num_ = g_->tune.cap_pct;
     cap_den_ = 100;
-    const uint32_t hub = g_->tune.hub_min_deg;
+    const uint32_t hub = g_->tune.hub_min_deg, dpw = g_->tune.dp_wmax, ssw = g_->tune.sssp_wmax;
+    const uint32_t mst = g_->tune.merge_stage;
+    persist_ = rounds_grid_ > 0 && g_->tune.persistent;
+    const uint32_t lw = persist_ ? rounds_grid_ * (256 / 32) : resident_light_warps_;
     CK(cudaMemcpyAsync(&d_rd_->hub_min_deg, &hub, sizeof(hub), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(&d_rd_->dp_wmax, &dpw, sizeof(dpw), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(&d_rd_->sssp_wmax, &ssw, sizeof(ssw), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(&d_rd_->merge_stage, &mst, sizeof(mst), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(&d_rd_->light_warps, &lw, sizeof(lw), cudaMemcpyHostToDevice, stream_));
     CK(cudaStreamSynchronize(stream_));
+    if (g_->tune.rounds_per_launch != rounds_per_sync_) {
+      rounds_per_sync_ = g_->tune.rounds_per_launch;
+      if (round_graph_) {
+        cudaGraphExecDestroy(round_graph_);
+        round_graph_ = nullptr;
+        gst_status gs = build_round_graph();
+        if (gs != GST_OK) return gs;
+      }
+    }
     return GST_OK;
   }
   size_t live() const { return n_used_; }
@@ -813,6 +852,35 @@ class Runner {
   gst_status launch_block(uint32_t R) {
     const int h = (int)(next_block_ & 1);
     const bool prof = g_->profile;
+    blk_persist_[h] = persist_ && !(prof && h_rdtrace_);  // the per-round trace needs separate launches
+    if (blk_persist_[h]) {
+      // the block's rounds as one persistent launch; its state is reset from
+      // this half's pinned template (rewritten only after the block of two
+      // launches ago was examined, so never under a copy in flight)
+      PersistCtl& tp = h_pc_[h];
+      memset(&tp, 0, sizeof(tp));
+      const uint32_t wm = g_->wait_ms.load();
+      tp.timeout_ns = (unsigned long long)(wm ? wm : wait_ms_default_) * 1000000ull;
+      tp.hold = g_->hold_rounds.load();
+      CK(cudaMemcpyAsync(d_pc_, &tp, sizeof(PersistCtl), cudaMemcpyHostToDevice, stream_));
+      GraphDev gd{g_->d_beg, g_->d_adj, g_->V, g_->d_wcut};
+      int nsc = (int)max_slots_;
+      uint32_t R32 = R;
+      PersistCtl* pc = d_pc_;
+      void* args[] = {&d_qd_, &d_ctl_, &nsc, &d_rd_, &d_pre_, &gd, &R32, &pc};
+      if (prof) CK(cudaEventRecord(ev_prof_[h][0], stream_));
+      CK(cudaLaunchCooperativeKernel((const void*)k_rounds, dim3(rounds_grid_), dim3(256), args, 0, stream_));
+      if (prof) CK(cudaEventRecord(ev_prof_[h][1], stream_));
+      CK(cudaMemcpyAsync(h_pc_ + 2 + h, d_pc_, sizeof(PersistCtl), cudaMemcpyDeviceToHost, stream_));
+      const int ns = (int)nslots_hi_;
+      prof_rounds_[h] = prof ? R : 0;
+      g_->launches += 1;
+      blk_slots_[h] = (uint32_t)ns;
+      CK(cudaMemcpyAsync(h_ctl_ + (size_t)h * MAX_SLOTS, d_ctl_, (size_t)ns * sizeof(QCtl), cudaMemcpyDeviceToHost,
+                         stream_));
+      CK(cudaEventRecord(ev_blk_[h], stream_));
+      return GST_OK;
+    }
     if (round_graph_ && R == rounds_per_sync_ && !prof) {
       CK(cudaGraphLaunch(round_graph_, stream_));
     } else {
@@ -844,6 +912,18 @@ class Runner {
   }
 
   void accumulate_profile(int h) {
+    if (blk_persist_[h]) {
+      // one launch for the block: its time goes to the round kernel (light),
+      // its rounds are those it ran with a live query
+      if (prof_rounds_[h]) {
+        float a = 0;
+        cudaEventElapsedTime(&a, ev_prof_[h][0], ev_prof_[h][1]);
+        g_->prof_light_ms += a;
+        g_->prof_rounds += h_pc_[2 + h].rounds;
+        g_->prof_persistent = true;
+      }
+      return;
+    }
     for (uint32_t r = 0; r < prof_rounds_[h]; r++) {
       float a = 0, b = 0;
       cudaEventElapsedTime(&a, ev_prof_[h][3 * r], ev_prof_[h][3 * r + 1]);
@@ -874,11 +954,16 @@ class Runner {
     const QCtl* snap = h_ctl_ + (size_t)h * MAX_SLOTS;
     char* estage = h_edge_stage_ + (size_t)h * (edge_stage_cap_ / 2);
     size_t off = 0;
+    // a persistent launch whose bounded wait expired left its queries' rounds
+    // unfinished: every query of the block that had not finished fails
+    const bool expired = blk_persist_[h] && h_pc_[2 + h].err != 0u;
+    if (expired) timeouts_++;
     for (uint32_t s = 0; s < blk_slots_[h]; s++) {
       Job* j = slots_[s];
-      if (!j || j->first_block > blk || !snap[s].done) continue;
+      if (!j || j->first_block > blk) continue;
+      if (!snap[s].done && !expired) continue;
       j->ctl = snap[s];
-      j->status = (gst_status)j->ctl.final_status;
+      j->status = snap[s].done ? (gst_status)j->ctl.final_status : GST_DEVICE_TIMEOUT;
       size_t my = (size_t)-1;
       if (j->status == GST_OK) {
         j->cost = (int32_t)(j->ctl.best_full >> 32);
@@ -958,6 +1043,12 @@ class Runner {
   size_t stage_cap_ = 0, stage_off_[2] = {0, 0}, edge_stage_cap_ = 0;
   int64_t next_block_ = 0;
   uint32_t blk_slots_[2] = {0, 0}, prof_rounds_[2] = {0, 0};
+  bool persist_ = false, blk_persist_[2] = {false, false};
+  unsigned rounds_grid_ = 0;  // blocks of the persistent launch (0: cooperative launch unavailable)
+  PersistCtl* d_pc_ = nullptr;
+  PersistCtl* h_pc_ = nullptr;  // pinned [4]: launch templates, then read-backs, per block half
+  uint32_t wait_ms_default_ = 30000;
+  uint64_t timeouts_ = 0;
   cudaEvent_t ev_blk_[2] = {nullptr, nullptr}, ev_fin_ = nullptr;
   cudaEvent_t ev_prof_[2][3 * 64] = {};
   RoundDesc* h_rdtrace_ = nullptr;  // pinned [2][64] round descriptors (GSTB_TRACE_ROUNDS)
@@ -1098,6 +1189,11 @@ gst_status gst_graph_create(const uint32_t* beg_pos, const uint32_t* csr, const 
   g->tune.delta_dp = std::max(1u, env_u32("GSTB_DELTA_DP", 8));
   g->tune.hub_min_deg = std::max(32u, env_u32("GSTB_HUB_MIN_DEG", 256));
   g->tune.cap_pct = std::min(100u, std::max(1u, env_u32("GSTB_SSSP_CAP_PCT", 60)));
+  g->tune.persistent = env_u32("GSTB_PERSIST", 0) ? 1u : 0u;
+  g->tune.rounds_per_launch = std::min(64u, std::max(1u, env_u32("GSTB_ROUNDS_PER_SYNC", 4)));
+  g->tune.dp_wmax = floor_pow2(std::min(32u, std::max(1u, env_u32("GSTB_DP_WMAX", 32))));
+  g->tune.sssp_wmax = floor_pow2(std::min(32u, std::max(4u, env_u32("GSTB_SSSP_WMAX", 32))));
+  g->tune.merge_stage = env_u32("GSTB_MERGE_STAGE", 0);
   cudaGetDevice(&g->device);
   cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device);
   {
@@ -1194,6 +1290,7 @@ void gst_profile_reset(gst_graph* g) {
   if (!g) return;
   g->prof_light_ms = g->prof_heavy_ms = 0;
   g->prof_rounds = 0;
+  g->prof_persistent = false;
   for (int t = 0; t < GST_NSTATS; t++) g->prof_stats[t] = 0;
 }
 
@@ -1223,8 +1320,10 @@ gst_status gst_tuning_get(gst_graph* g, gst_tuning* out) {
 }
 
 gst_status gst_tuning_set(gst_graph* g, const gst_tuning* t) {
+  auto pow2_in = [](uint32_t x, uint32_t lo, uint32_t hi) { return x >= lo && x <= hi && (x & (x - 1)) == 0; };
   if (!g || !t || t->delta_sssp < 1 || t->delta_dp < 1 || t->hub_min_deg < 32 || t->cap_pct < 1 ||
-      t->cap_pct > 100)
+      t->cap_pct > 100 || t->persistent > 1 || t->rounds_per_launch < 1 || t->rounds_per_launch > 64 ||
+      !pow2_in(t->dp_wmax, 1, 32) || !pow2_in(t->sssp_wmax, 4, 32))
     return GST_BAD_INPUT;
   std::lock_guard<std::mutex> lock(g->mu);
   g->tune = *t;
@@ -1385,18 +1484,26 @@ gst_status gst_autotune(gst_graph* g, int n, const uint32_t* groups, const int32
   st = measure(best_ms);
   if (st != GST_OK) return st;
   // one parameter at a time over a few candidates each
-  const uint32_t cands[4][4] = {{50, 60, 67, 75}, {8, 16, 32, 64}, {2, 4, 8, 16}, {128, 256, 512, 1024}};
-  auto field_of = [](gst_tuning& t, int param) -> uint32_t& {
-    return param == 0 ? t.cap_pct : (param == 1 ? t.delta_sssp : (param == 2 ? t.delta_dp : t.hub_min_deg));
+  struct Cand {
+    uint32_t gst_tuning::*field;
+    std::vector<uint32_t> vals;
   };
-  for (int param = 0; param < 4; param++) {
-    const uint32_t* cand = cands[param];
-    for (int c = 0; c < 4; c++) {
+  const Cand cands[] = {
+      {&gst_tuning::cap_pct, {50, 60, 67, 75}},
+      {&gst_tuning::delta_sssp, {8, 16, 32, 64}},
+      {&gst_tuning::delta_dp, {2, 4, 8, 16}},
+      {&gst_tuning::hub_min_deg, {128, 256, 512, 1024}},
+      {&gst_tuning::persistent, {0, 1}},
+      {&gst_tuning::rounds_per_launch, {2, 4, 8, 16}},
+      {&gst_tuning::dp_wmax, {4, 8, 16, 32}},
+      {&gst_tuning::sssp_wmax, {8, 16, 32}},
+      {&gst_tuning::merge_stage, {0, 6, 14, 30}},
+  };
+  for (const Cand& cd : cands) {
+    for (uint32_t v : cd.vals) {
+      if (v == cur.*cd.field) continue;
       gst_tuning t = cur;
-      uint32_t& field = field_of(t, param);
-      const uint32_t now = field_of(cur, param);
-      if (cand[c] == now) continue;
-      field = cand[c];
+      t.*cd.field = v;
       if ((st = gst_tuning_set(g, &t)) != GST_OK) return st;
       double ms = 0;
       if ((st = measure(ms)) != GST_OK) return st;
@@ -1656,6 +1763,13 @@ gst_status gst_debug_fail_allocs(gst_graph* g, int n) {
   return GST_OK;
 }
 
+gst_status gst_debug_hold_rounds(gst_graph* g, int hold, uint32_t timeout_ms) {
+  if (!g || hold < 0 || hold > 1) return GST_BAD_INPUT;
+  g->wait_ms.store(timeout_ms);
+  g->hold_rounds.store((uint32_t)hold);
+  return GST_OK;
+}
+
 gst_status gst_serve_close(gst_server* S) {
   if (!S) return GST_BAD_INPUT;
   {
@@ -1812,7 +1926,9 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
     memset(&rd0, 0, sizeof(rd0));
     rd0.light_warps = light_grid * (256 / 32);
     rd0.sssp_w = 4;
-    rd0.dp_wmax = std::min(32u, std::max(1u, env_u32("GSTB_DP_WMAX", 32)));
+    rd0.dp_wmax = g->tune.dp_wmax;
+    rd0.sssp_wmax = g->tune.sssp_wmax;
+    rd0.merge_stage = g->tune.merge_stage;
     CK(cudaMemcpy(d_rd, &rd0, sizeof(RoundDesc), cudaMemcpyHostToDevice));
   }
   // member items v*8 + j, staged through a fixed host array (calls are

@@ -288,7 +288,7 @@ __device__ __forceinline__ void grow_arcs(const QDev& q, const GraphDev& g, uint
       ok[u] = ok[u] && arc[u].y <= lim;
       const uint32_t vp = (arc[u].x << k) | p;
       t[u] = dnext < 0 ? vp : vp * nd + (uint32_t)dnext;
-      lbu[u] = ok[u] ? (uint32_t)__ldg(lbt + ((size_t)arc[u].x << k) + comp) : 0u;
+      lbu[u] = ok[u] ? (uint32_t)ld_round(lbt + ((size_t)arc[u].x << k) + comp) : 0u;
     }
     bool any = false;
 #pragma unroll
@@ -370,7 +370,7 @@ __device__ __forceinline__ void load_dl(const QDev& q, uint32_t v, uint32_t (&dl
                                         uint32_t& raw_sum_ok, uint32_t comp,
                                         unsigned long long& raw_sum) {
   const uint4* row = reinterpret_cast<const uint4*>(q.dist + (size_t)v * 8);
-  uint4 a = __ldg(row), b = __ldg(row + 1);
+  uint4 a = ld_round(row), b = ld_round(row + 1);
   uint32_t r[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
   raw_sum = 0;
   raw_sum_ok = 1;
@@ -409,6 +409,13 @@ __device__ __forceinline__ uint32_t find_slot_s(const uint32_t* pre, int nslots,
   }
   return (uint32_t)lo;
 }
+
+// A DP state's vertex row staged for its merges: the costs of its 2^k table
+// entries and its 2^k bound-table entries.
+struct MergeTile {
+  uint32_t cost[1u << KMAX];
+  unsigned short lb[1u << KMAX];
+};
 
 // ---------------------------------------------------------------------------
 // Unbounded DP item (v, p), in two parts.  dp_gate runs on one lane for its
@@ -461,14 +468,14 @@ __device__ __forceinline__ bool dp_gate(const QDev& q, uint32_t s, uint32_t& c_o
     }
   }
   counted = true;
-  const uint32_t lbv = __ldg(q.lbt + ((size_t)v << k) + comp);
+  const uint32_t lbv = ld_round(q.lbt + ((size_t)v << k) + comp);
   c_out = c;
   best_out = best;
   return lb_ok(c, lbv, best);
 }
 
 __device__ void dp_expand(const QDev& q, const GraphDev& g, uint32_t s, uint32_t c, uint32_t best, uint32_t lane,
-                          RoundDesc* __restrict__ rd, uint32_t slot, WarpStat& ws, WarpBuf& wb) {
+                          RoundDesc* __restrict__ rd, uint32_t slot, WarpStat& ws, WarpBuf& wb, MergeTile* mt) {
   const int k = q.k;
   const uint32_t K2 = 1u << k, full = (uint32_t)q.full;
   const uint32_t v = s >> k, p = s & (K2 - 1u), comp = full ^ p;
@@ -488,10 +495,25 @@ __device__ void dp_expand(const QDev& q, const GraphDev& g, uint32_t s, uint32_t
     grow_arcs(q, g, lane, v, p, comp, c, best, lim, -1, a0, a1, gc, wb);
   }
   // merge with every proper, non-empty subset p2 of the complement
-  // (DPQ.cu:140-170; the complement itself went to the full state above)
+  // (DPQ.cu:140-170; the complement itself went to the full state above).
+  // Lane j takes the subsets idx = j, j+32, .. (p2 = the idx+1-th subset of
+  // the complement, by bit deposit); a state with many partners first stages
+  // its vertex's costs and bound row in shared memory with coalesced loads,
+  // so every partner is read from there.  A staged cost can be higher than
+  // the table's by then (another warp lowered it): a partner missed that way
+  // merges with this state when it is expanded itself, and a target whose
+  // cost only looked higher gets a min that changes nothing.
   uint32_t merges = 0;
   {
     const uint32_t nsub = (1u << __popc(comp)) - 2u;
+    const bool staged = mt != nullptr && rd->merge_stage != 0u && nsub >= rd->merge_stage;
+    if (staged) {
+      for (uint32_t i = lane; i < K2; i += 32u) {
+        mt->cost[i] = (uint32_t)(ld_cg(row + i) >> 32);
+        mt->lb[i] = ld_round(lbt + ((size_t)v << k) + i);
+      }
+      __syncwarp();
+    }
     for (uint32_t b = 0; b < nsub; b += 32) {
       uint32_t idx = b + lane;
       bool want = false;
@@ -499,14 +521,14 @@ __device__ void dp_expand(const QDev& q, const GraphDev& g, uint32_t s, uint32_t
       if (idx < nsub) {
         uint32_t p2 = pdep(idx + 1u, comp);
         uint32_t qset = p | p2;
-        uint32_t c2 = (uint32_t)(ld_cg(row + p2) >> 32);
-        uint32_t cq = (uint32_t)(ld_cg(row + qset) >> 32);
+        uint32_t c2 = staged ? mt->cost[p2] : (uint32_t)(ld_cg(row + p2) >> 32);
+        uint32_t cq = staged ? mt->cost[qset] : (uint32_t)(ld_cg(row + qset) >> 32);
         if (c2 != INF32) {
           merges++;
           unsigned long long m = (unsigned long long)c + c2;
           // conditional tree merging: 3m <= 2 best (CPUNONHOP.h:941)
           if (3ull * m <= 2ull * best && m < cq) {
-            uint32_t lbq = __ldg(lbt + ((size_t)v << k) + (full ^ qset));
+            uint32_t lbq = staged ? (uint32_t)mt->lb[full ^ qset] : ld_round(lbt + ((size_t)v << k) + (full ^ qset));
             if (lb_ok((uint32_t)m, lbq, best)) {
               m32 = (uint32_t)m;
               t = (v << k) | qset;
@@ -519,6 +541,7 @@ __device__ void dp_expand(const QDev& q, const GraphDev& g, uint32_t s, uint32_t
       }
       gc.enq += enqueue_warp(want, t, m32, q, lane, wb);
     }
+    if (staged) __syncwarp();  // the tile is free for the next state
   }
   const uint32_t sa = warp_sum(gc.arcs), su = warp_sum(gc.upd), se = warp_sum(gc.enq), sm = warp_sum(merges);
   if (lane == 0) {
@@ -559,7 +582,7 @@ __device__ __forceinline__ bool hop_gate(const QDev& q, uint32_t s, uint32_t& c_
   const uint32_t lbh = hop_budget_one(q, v, comp, (uint32_t)D - d);
   if (lbh == INF32 || (unsigned long long)c + lbh > best) return false;
   counted = true;
-  const uint32_t lbv = __ldg(q.lbt + ((size_t)v << k) + comp);
+  const uint32_t lbv = ld_round(q.lbt + ((size_t)v << k) + comp);
   c_out = c;
   best_out = best;
   return lb_ok(c, lbv, best);
@@ -614,7 +637,7 @@ __device__ void hop_expand(const QDev& q, const GraphDev& g, uint32_t s, uint32_
               atomicMin(&q.ctl->best_full, ((unsigned long long)m32 << 32) | (v * 8u + ndd));
               if (m32 < best) atomicMin(&q.ctl->best, m32);
             } else {
-              uint32_t lbq = __ldg(lbt + ((size_t)v << k) + (full ^ qset));
+              uint32_t lbq = ld_round(lbt + ((size_t)v << k) + (full ^ qset));
               if (lb_ok(m32, lbq, best) && m32 < (uint32_t)(ld_cg(q.table + t) >> 32)) {
                 red_min(q.table + t, pack(m32, par));
                 want = true;
@@ -641,9 +664,9 @@ __device__ void hop_expand(const QDev& q, const GraphDev& g, uint32_t s, uint32_
 // states one after another.  W is chosen per round by k_control (1 when the
 // round has few items, so that each state gets a warp of its own; up to 32
 // when it has many, most of which the gates drop).
-__device__ void dp_task(const QDev* __restrict__ qd, const uint32_t* __restrict__ pre, int nslots, uint32_t total,
+__device__ void dp_task(const QDev* qd, const uint32_t* __restrict__ pre, int nslots, uint32_t total,
                         uint32_t task, uint32_t W, bool hop, const GraphDev& g, uint32_t lane,
-                        RoundDesc* __restrict__ rd, WarpStat& ws, WarpBuf& wb) {
+                        RoundDesc* __restrict__ rd, WarpStat& ws, WarpBuf& wb, MergeTile* mt) {
   const unsigned FULL = 0xFFFFFFFFu;
   const uint32_t it = task * W + lane;
   const bool valid = lane < W && it < total;
@@ -673,7 +696,7 @@ __device__ void dp_task(const QDev* __restrict__ qd, const uint32_t* __restrict_
     if (hop)
       hop_expand(q, g, ss, cc, bb, lane, rd, si, ws, wb);
     else
-      dp_expand(q, g, ss, cc, bb, lane, rd, si, ws, wb);
+      dp_expand(q, g, ss, cc, bb, lane, rd, si, ws, wb, mt);
   }
 }
 
@@ -714,6 +737,15 @@ struct alignas(16) RelaxHdr {
 
 struct RelaxCnt {
   uint32_t arcs = 0, upd = 0, enq = 0;
+};
+
+// Per-warp shared scratch; a warp uses one member at a time: the headers of
+// its distance items (or of a hub chunk), its bound rows' capped distances,
+// or a DP state's merge tile.
+union WarpScratch {
+  RelaxHdr hdr[32];
+  uint32_t dl[KMAX][32];
+  MergeTile mg;
 };
 
 __device__ __forceinline__ uint32_t sel8(const uint4& a, const uint4& b, uint32_t i) {
@@ -837,7 +869,7 @@ __device__ __forceinline__ void relax_cnt_add(WarpStat& ws, QCtl* c, RelaxCnt cn
   }
 }
 
-__device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restrict__ pre, int nslots,
+__device__ void sssp_task(const QDev* qd, const uint32_t* __restrict__ pre, int nslots,
                           uint32_t total, uint32_t task, uint32_t W, const GraphDev& g, uint32_t lane, WarpStat& ws,
                           RoundDesc* __restrict__ rd, RelaxHdr* __restrict__ sh, WarpBuf& wb) {
   const unsigned FULL = 0xFFFFFFFFu;
@@ -966,7 +998,7 @@ __device__ void sssp_task(const QDev* __restrict__ qd, const uint32_t* __restric
 
 // One hub chunk (k_heavy, one warp): relax arcs [first, end) of vertex v for
 // the pending groups recorded by k_light.  Same relaxation as sssp_task.
-__device__ void hub_chunk(const QDev* __restrict__ qd, const uint4 item, const GraphDev& g, uint32_t lane,
+__device__ void hub_chunk(const QDev* qd, const uint4 item, const GraphDev& g, uint32_t lane,
                           RelaxHdr* __restrict__ sh, WarpStat& ws, WarpBuf& wb) {
   const unsigned FULL = 0xFFFFFFFFu;
   if (item.z >= item.w) return;  // filler entry of a chunk run that did not fit
@@ -1009,7 +1041,7 @@ __device__ void hub_chunk(const QDev* __restrict__ qd, const uint4 item, const G
 // k_light warp handed over.  The state's current cost is read again (it can
 // only have dropped, and a lower cost grows validly too) and the gates of the
 // state's own expansion are re-checked.
-__device__ void grow_chunk(const QDev* __restrict__ qd, const uint4 item, const GraphDev& g, uint32_t lane,
+__device__ void grow_chunk(const QDev* qd, const uint4 item, const GraphDev& g, uint32_t lane,
                            WarpStat& ws, WarpBuf& wb) {
   const unsigned FULL = 0xFFFFFFFFu;
   if (item.z >= item.w) return;  // filler entry of a chunk run that did not fit
@@ -1024,7 +1056,7 @@ __device__ void grow_chunk(const QDev* __restrict__ qd, const uint4 item, const 
   if (lane == 0) {
     c = (uint32_t)(ld_cg(q.table + s) >> 32);
     best = ld_best(q.ctl);
-    lbv = __ldg(q.lbt + ((size_t)v << k) + comp);
+    lbv = ld_round(q.lbt + ((size_t)v << k) + comp);
   }
   c = __shfl_sync(FULL, c, 0);
   best = __shfl_sync(FULL, best, 0);
@@ -1220,17 +1252,17 @@ __device__ __forceinline__ uint32_t lower_bound_uniform(const uint32_t (*sdl)[32
     const uint32_t* Pi = P + ((size_t)i * K2 + X) * k;
     for (uint32_t mj = mi & (mi - 1u); mj; mj &= mj - 1u) {  // the groups of X above i
       const uint32_t j = __ffs(mj) - 1;
-      const uint32_t pij = min(__ldg(Pi + j), __ldg(P + ((size_t)j * K2 + X) * k + i));
+      const uint32_t pij = min(ld_round(Pi + j), ld_round(P + ((size_t)j * K2 + X) * k + i));
       m1 = min(m1, di + pij + sdl[j][lane]);
     }
-    m2 = max(m2, di + __ldg(T2 + (size_t)i * K2 + X) + mind);
+    m2 = max(m2, di + ld_round(T2 + (size_t)i * K2 + X) + mind);
   }
   const uint32_t lb1 = (min(m1, BIG) + 1u) >> 1;
   const uint32_t lb2 = (min(m2, BIG) + 1u) >> 1;
   return max(lb0, max(lb1, lb2));
 }
 
-__device__ void lbt_rows32(const QDev* __restrict__ qd, const uint32_t* __restrict__ pre, int nslots, uint32_t n_lb,
+__device__ void lbt_rows32(const QDev* qd, const uint32_t* __restrict__ pre, int nslots, uint32_t n_lb,
                            uint32_t task, uint32_t lane, uint32_t (*sdl)[32]) {
   const unsigned FULL = 0xFFFFFFFFu;
   const uint32_t it = task * 32u + lane;
@@ -1253,8 +1285,8 @@ __device__ void lbt_rows32(const QDev* __restrict__ qd, const uint32_t* __restri
       uint4 a = make_uint4(0u, 0u, 0u, 0u), b = a;
       if (mine) {
         const uint4* row = reinterpret_cast<const uint4*>(q.dist + (size_t)v * ROW);
-        a = __ldg(row);
-        b = __ldg(row + 1);
+        a = ld_round(row);
+        b = ld_round(row + 1);
       }
       const uint32_t r[KMAX] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z};
 #pragma unroll
@@ -1617,24 +1649,34 @@ __device__ __forceinline__ void decide(QDev& q, QCtl& c) {
   }
 }
 
-__global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* __restrict__ ctl, int nslots,
-                                                  RoundDesc* __restrict__ rd, uint32_t* __restrict__ pre) {
-  __shared__ uint32_t wsum[32][NT];
-  __shared__ uint32_t live_cnt, used_hi;
-  const int tid = threadIdx.x;
-  const uint32_t lane = tid & 31, wid = tid >> 5;
-  if (tid == 0) live_cnt = used_hi = 0;
+// Shared memory of one control step.
+struct CtlSmem {
+  uint32_t wsum[32][NT];  // per-warp inclusive totals, then their scan
+  uint32_t carry[NT];     // items of the slots in earlier chunks
+  uint32_t live_cnt, used_hi;
+};
+
+// One control step over slots [0, nslots) by all threads of one block
+// (blockDim.x a multiple of 32, at most 1024).  Slots go in chunks of
+// blockDim.x; the per-type prefixes carry from one chunk to the next, so any
+// block size gives the same prefixes.
+__device__ void control_step(QDev* qd, QCtl* ctl, int nslots, RoundDesc* rd, uint32_t* pre, CtlSmem& sm) {
+  const int tid = threadIdx.x, B = blockDim.x;
+  const uint32_t lane = tid & 31, wid = tid >> 5, nw = (uint32_t)B >> 5;
+  if (tid == 0) sm.live_cnt = sm.used_hi = 0;
+  if (tid < NT) sm.carry[tid] = 0;
   __syncthreads();
-  uint32_t cnt[NT];
+  for (int base = 0; base <= nslots; base += B) {
+    const int s = base + tid;
+    uint32_t cnt[NT];
 #pragma unroll
-  for (int t = 0; t < NT; t++) cnt[t] = 0;
-  // the state alone first: most slots are free when the scan covers them all
-  const int32_t st0 = tid < nslots ? qd[tid].st : J_FREE;
-  if (st0 != J_FREE) atomicMax(&used_hi, (uint32_t)tid + 1u);
-  if (st0 != J_FREE && st0 != J_DONE) {
-    QDev q = qd[tid];
-    QCtl& c = ctl[tid];
-    {
+    for (int t = 0; t < NT; t++) cnt[t] = 0;
+    // the state alone first: most slots are free when the scan covers them all
+    const int32_t st0 = s < nslots ? qd[s].st : J_FREE;
+    if (st0 != J_FREE) atomicMax(&sm.used_hi, (uint32_t)s + 1u);
+    if (st0 != J_FREE && st0 != J_DONE) {
+      QDev q = qd[s];
+      QCtl& c = ctl[s];
       absorb(q, c);
       if (q.st != J_DONE) decide(q, c);
       switch (q.act) {
@@ -1650,61 +1692,63 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
         default: break;
       }
       if (q.snap_h) cnt[T_SNAP] = q.nv;  // copy the distance rows of round snap_h
-      if (q.st != J_DONE) atomicAdd(&live_cnt, 1u);
-      qd[tid] = q;
+      if (q.st != J_DONE) atomicAdd(&sm.live_cnt, 1u);
+      qd[s] = q;
     }
-  }
-  // exclusive scan over slots, per task type
-  uint32_t incl[NT];
-#pragma unroll
-  for (int t = 0; t < NT; t++) {
-    uint32_t x = cnt[t];
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-      if (lane >= (uint32_t)o) x += y;
-    }
-    incl[t] = x;
-    if (lane == 31) wsum[wid][t] = x;
-  }
-  __syncthreads();
-  if (wid == 0) {
+    // exclusive scan over the chunk's slots, per task type
+    uint32_t incl[NT];
 #pragma unroll
     for (int t = 0; t < NT; t++) {
-      uint32_t x = lane < (blockDim.x >> 5) ? wsum[lane][t] : 0u;
+      uint32_t x = cnt[t];
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
         if (lane >= (uint32_t)o) x += y;
       }
-      wsum[lane][t] = x;  // inclusive over warps
+      incl[t] = x;
+      if (lane == 31) sm.wsum[wid][t] = x;
     }
-  }
-  __syncthreads();
+    __syncthreads();
+    if (wid == 0) {
 #pragma unroll
-  for (int t = 0; t < NT; t++) {
-    uint32_t before = (wid ? wsum[wid - 1][t] : 0u) + incl[t] - cnt[t];
-    if (tid <= nslots) pre[t * (MAX_SLOTS + 1) + tid] = before;
+      for (int t = 0; t < NT; t++) {
+        uint32_t x = lane < nw ? sm.wsum[lane][t] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+          if (lane >= (uint32_t)o) x += y;
+        }
+        sm.wsum[lane][t] = x;  // inclusive over warps
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+      uint32_t before = sm.carry[t] + (wid ? sm.wsum[wid - 1][t] : 0u) + incl[t] - cnt[t];
+      if (s <= nslots) pre[t * (MAX_SLOTS + 1) + s] = before;
+    }
+    __syncthreads();  // carry and wsum read by every thread
+    if (tid < NT) sm.carry[tid] += sm.wsum[nw - 1][tid];
+    __syncthreads();
   }
   if (tid == 0) {
     // distance items per warp task: 4 while that leaves at most two tasks per
-    // light warp, more (up to 32) in rounds with many items
+    // light warp, more (up to sssp_wmax) in rounds with many items
     uint32_t w = 4;
-    const unsigned long long n_sssp = wsum[(blockDim.x >> 5) - 1][T_SSSP];
-    while (w < SSSP_WMAX && n_sssp > 2ull * w * rd->light_warps) w <<= 1;
+    const unsigned long long n_sssp = sm.carry[T_SSSP];
+    while (w < min(rd->sssp_wmax, SSSP_WMAX) && n_sssp > 2ull * w * rd->light_warps) w <<= 1;
     rd->sssp_w = w;
     // DP states per warp task: 1 while that leaves at most two tasks per
-    // light warp (every state gets a warp), more (up to 32) in rounds with
-    // many states
+    // light warp (every state gets a warp), more (up to dp_wmax) in rounds
+    // with many states
     uint32_t wd = 1;
-    const unsigned long long n_dp = (unsigned long long)wsum[(blockDim.x >> 5) - 1][T_DP] +
-                                    wsum[(blockDim.x >> 5) - 1][T_HOP];
+    const unsigned long long n_dp = (unsigned long long)sm.carry[T_DP] + sm.carry[T_HOP];
     while (wd < rd->dp_wmax && n_dp > 2ull * wd * rd->light_warps) wd <<= 1;
     rd->dp_w = wd;
     const uint32_t per_task[NT] = {32, 32, 32, 1, 1, w, wd, wd, 32, 32};
     uint32_t off = 0;
     for (int t = 0; t < NT; t++) {
-      uint32_t tot = wsum[(blockDim.x >> 5) - 1][t];
+      uint32_t tot = sm.carry[t];
       rd->items[t] = tot;
       if (t == T_LB) {
         rd->light_tasks = off;
@@ -1715,8 +1759,8 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
     }
     rd->task_off[NT] = off;
     rd->heavy_tasks = off;
-    rd->n_live = live_cnt;
-    rd->nslots = used_hi;  // slots the round kernels search (all later ones are free)
+    rd->n_live = sm.live_cnt;
+    rd->nslots = sm.used_hi;  // slots the round kernels search (all later ones are free)
     rd->n_big = 0;
     rd->next_light = 0;
     rd->next_heavy = 0;
@@ -1730,10 +1774,115 @@ __global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* _
   }
 }
 
+__global__ void __launch_bounds__(1024) k_control(QDev* __restrict__ qd, QCtl* __restrict__ ctl, int nslots,
+                                                  RoundDesc* __restrict__ rd, uint32_t* __restrict__ pre) {
+  __shared__ CtlSmem sm;
+  control_step(qd, ctl, nslots, rd, pre, sm);
+}
+
 // ---------------------------------------------------------------------------
-// Light round kernel: warp tasks of types T_SPLIT .. T_HOP (splits, seeds,
-// tour tables, extraction, distance items, DP states).
+// Round work, one warp task at a time.  The separate round kernels (k_light,
+// k_heavy) and the persistent one (k_rounds) run the same tasks.
 // ---------------------------------------------------------------------------
+
+// Light task `task` (types T_SPLIT .. T_HOP: splits, seeds, tour tables,
+// extraction, distance items, DP states).  s_pre / s_dp / s_hop: the per-slot
+// prefixes of the distance, DP and hop items, staged in shared memory.
+__device__ __forceinline__ void light_task(const QDev* qd, RoundDesc* rd, const uint32_t* pre,
+                                           const uint32_t* s_pre, const uint32_t* s_dp, const uint32_t* s_hop,
+                                           int nslots, const GraphDev& g, uint32_t task, uint32_t lane,
+                                           WarpStat& ws, WarpBuf& wb, WarpScratch& sc) {
+  int t = 0;
+  while (t < T_HOP && task >= __ldcg(&rd->task_off[t + 1])) t++;
+  const uint32_t local = task - __ldcg(&rd->task_off[t]);
+  const uint32_t* P = pre + t * (MAX_SLOTS + 1);
+  const uint32_t total = __ldcg(&rd->items[t]);
+  if (t == T_SSSP) {
+    sssp_task(qd, s_pre, nslots, total, local, __ldcg(&rd->sssp_w), g, lane, ws, rd, sc.hdr, wb);
+  } else if (t == T_DP || t == T_HOP) {
+    dp_task(qd, t == T_DP ? s_dp : s_hop, nslots, total, local, __ldcg(&rd->dp_w), t == T_HOP, g, lane, rd, ws, wb,
+            &sc.mg);
+  } else if (t == T_TOUR) {
+    tour_warp(qd[find_slot(P, nslots, local)], lane);
+  } else if (t == T_EXTRACT) {
+    extract_warp(qd[find_slot(P, nslots, local)], g, lane);
+  } else {
+    const uint32_t it = local * 32u + lane;
+    bool toN = false, toF = false;
+    uint32_t slot = 0, item = 0;
+    if (it < total) {
+      slot = find_slot(P, nslots, it);
+      const QDev& q = qd[slot];
+      const uint32_t idx = it - __ldcg(P + slot);
+      if (t == T_SPLIT) {
+        item = q.qbuf[q.far_idx][idx];
+        split_item(q, item, toN, toF);
+      } else if (t == T_SSEED) {
+        const uint32_t m = __ldg(q.members + idx);
+        item = m >> 3;
+        sseed_item(q, m, toN);
+      } else {
+        dseed_item(q, __ldg(q.members + idx));
+      }
+    }
+    push_multi(toN, item, 0u, qd[slot], slot, lane);
+    push_multi(toF, item, 1u, qd[slot], slot, lane);
+  }
+}
+
+// Heavy task `ht` that does not depend on the round's light tasks: bound-table
+// rows (one vertex per lane) and snapshot rows of hop-bounded queries.
+__device__ __forceinline__ void heavy_static_task(const QDev* qd, const uint32_t* pre, const uint32_t* s_lb,
+                                                  int nslots, uint32_t ht, uint32_t snap0, uint32_t n_lb,
+                                                  uint32_t n_snap, uint32_t lane, uint32_t (*sdl)[32]) {
+  if (ht < snap0) {
+    lbt_rows32(qd, s_lb, nslots, n_lb, ht, lane, sdl);
+    return;
+  }
+  // snapshot of a hop-bounded query's distance rows, one row per lane
+  const uint32_t it = (ht - snap0) * 32u + lane;
+  if (it < n_snap) {
+    const uint32_t* P = pre + T_SNAP * (MAX_SLOTS + 1);
+    const uint32_t slot = find_slot(P, nslots, it);
+    const QDev& qs = qd[slot];
+    const uint32_t v = it - __ldcg(P + slot);
+    const uint4* src = reinterpret_cast<const uint4*>(qs.dist + (size_t)v * ROW);
+    uint4* dst = reinterpret_cast<uint4*>(qs.snap + ((size_t)(qs.snap_h - 1u) * qs.nv + v) * ROW);
+    const uint4 a = __ldcg(src), b = __ldcg(src + 1);
+    dst[0] = a;
+    dst[1] = b;
+    if (qs.snap_h == qs.star_h || qs.snap_h == qs.center_h) {
+      // the rows are the exact distances over paths of at most snap_h hops
+      const uint32_t r[KMAX] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z};
+      bool all = true;
+      unsigned long long sum = 0;
+#pragma unroll
+      for (int t = 0; t < KMAX; t++)
+        if (t < qs.k) {
+          all = all && r[t] != INF32;
+          sum += r[t];
+        }
+      if (all && qs.snap_h == qs.center_h && __ldca(&qs.ctl->center) == 0u) atomicExch(&qs.ctl->center, 1u);
+      // v joined to every group by its cheapest path of at most star_h
+      // hops: a breadth-first tree from v inside their union has depth <=
+      // star_h, so diameter <= 2 * star_h <= D, at cost <= sum
+      if (all && qs.snap_h == qs.star_h && sum < ld_best(qs.ctl)) atomicMin(&qs.ctl->best, (uint32_t)sum);
+    }
+  }
+}
+
+// Arc chunk `i` that a light task handed over this round (hub vertex of a
+// distance item, or a high-degree DP state's grow).
+__device__ __forceinline__ void chunk_task(const QDev* qd, const RoundDesc* rd, const GraphDev& g, uint32_t i,
+                                           uint32_t lane, RelaxHdr* hub, WarpStat& ws, WarpBuf& wb) {
+  const uint4 it = __ldcg(rd->big + i);
+  if (it.x & CH_GROW)
+    grow_chunk(qd, it, g, lane, ws, wb);
+  else
+    hub_chunk(qd, it, g, lane, hub, ws, wb);
+}
+
+// Light round kernel: the round's light tasks.
 #ifndef GSTB_LIGHT_MIN_BLOCKS
 #define GSTB_LIGHT_MIN_BLOCKS 3
 #endif
@@ -1746,7 +1895,7 @@ __global__ void __launch_bounds__(256, GSTB_LIGHT_MIN_BLOCKS) k_light(const QDev
   nslots = min(nslots, (int)__ldcg(&rd->nslots));
   // prefixes over slots of the item types with many items, staged once per block
   __shared__ uint32_t s_pre[MAX_SLOTS + 1], s_dp[MAX_SLOTS + 1], s_hop[MAX_SLOTS + 1];
-  __shared__ RelaxHdr s_hdr[8][SSSP_WMAX];
+  __shared__ WarpScratch s_sc[8];
   __shared__ WarpStat s_ws[8];
   __shared__ WarpBuf s_wb[8];
   WarpStat& ws = s_ws[threadIdx.x >> 5];
@@ -1762,54 +1911,17 @@ __global__ void __launch_bounds__(256, GSTB_LIGHT_MIN_BLOCKS) k_light(const QDev
   }
   __syncthreads();
 #if GSTB_STEAL
-  for (uint32_t task = warp; task < ntasks; task = next_task(&rd->next_light, nwarps, lane)) {
+  for (uint32_t task = warp; task < ntasks; task = next_task(&rd->next_light, nwarps, lane))
 #else
-  for (uint32_t task = warp; task < ntasks; task += nwarps) {
+  for (uint32_t task = warp; task < ntasks; task += nwarps)
 #endif
-    int t = 0;
-    while (t < T_HOP && task >= __ldcg(&rd->task_off[t + 1])) t++;
-    const uint32_t local = task - __ldcg(&rd->task_off[t]);
-    const uint32_t* P = pre + t * (MAX_SLOTS + 1);
-    const uint32_t total = __ldcg(&rd->items[t]);
-    if (t == T_SSSP) {
-      sssp_task(qd, s_pre, nslots, total, local, __ldcg(&rd->sssp_w), g, lane, ws, rd, s_hdr[threadIdx.x >> 5], wb);
-    } else if (t == T_DP || t == T_HOP) {
-      dp_task(qd, t == T_DP ? s_dp : s_hop, nslots, total, local, __ldcg(&rd->dp_w), t == T_HOP, g, lane, rd, ws,
-              wb);
-    } else if (t == T_TOUR) {
-      tour_warp(qd[find_slot(P, nslots, local)], lane);
-    } else if (t == T_EXTRACT) {
-      extract_warp(qd[find_slot(P, nslots, local)], g, lane);
-    } else {
-      const uint32_t it = local * 32u + lane;
-      bool toN = false, toF = false;
-      uint32_t slot = 0, item = 0;
-      if (it < total) {
-        slot = find_slot(P, nslots, it);
-        const QDev& q = qd[slot];
-        const uint32_t idx = it - __ldcg(P + slot);
-        if (t == T_SPLIT) {
-          item = q.qbuf[q.far_idx][idx];
-          split_item(q, item, toN, toF);
-        } else if (t == T_SSEED) {
-          const uint32_t m = __ldg(q.members + idx);
-          item = m >> 3;
-          sseed_item(q, m, toN);
-        } else {
-          dseed_item(q, __ldg(q.members + idx));
-        }
-      }
-      push_multi(toN, item, 0u, qd[slot], slot, lane);
-      push_multi(toF, item, 1u, qd[slot], slot, lane);
-    }
-  }
+    light_task(qd, rd, pre, s_pre, s_dp, s_hop, nslots, g, task, lane, ws, wb, s_sc[threadIdx.x >> 5]);
   wb_flush(wb, lane);
   if (lane == 0) ws_flush(ws);
 }
 
-// Heavy round kernel: the arc chunks k_light handed over this round (hub
-// vertices of distance items, high-degree DP states), then lower-bound table
-// rows (8 lanes per vertex).
+// Heavy round kernel: the arc chunks k_light handed over this round, then
+// bound-table rows and snapshot rows.
 __global__ void __launch_bounds__(256, 3) k_heavy(const QDev* __restrict__ qd, RoundDesc* __restrict__ rd,
                                                const uint32_t* __restrict__ pre, int nslots, GraphDev g) {
   const uint32_t lane = threadIdx.x & 31u;
@@ -1838,52 +1950,150 @@ __global__ void __launch_bounds__(256, 3) k_heavy(const QDev* __restrict__ qd, R
 #else
   for (uint32_t task = warp; task < ntasks; task += nwarps) {
 #endif
-    if (task < nbig) {
-      const uint4 it = __ldcg(rd->big + task);
-      if (it.x & CH_GROW)
-        grow_chunk(qd, it, g, lane, ws, wb);
-      else
-        hub_chunk(qd, it, g, lane, &s_hub[threadIdx.x >> 5], ws, wb);
-      continue;
-    }
-    const uint32_t ht = task - nbig;
-    if (ht < snap0) {  // lower-bound table rows, one vertex per lane
-      lbt_rows32(qd, s_lb, nslots, n_lb, ht, lane, s_dl[threadIdx.x >> 5]);
-      continue;
-    }
-    // snapshot of a hop-bounded query's distance rows, one row per lane
-    const uint32_t it = (ht - snap0) * 32u + lane;
-    if (it < n_snap) {
-      const uint32_t* P = pre + T_SNAP * (MAX_SLOTS + 1);
-      const uint32_t slot = find_slot(P, nslots, it);
-      const QDev& qs = qd[slot];
-      const uint32_t v = it - __ldcg(P + slot);
-      const uint4* src = reinterpret_cast<const uint4*>(qs.dist + (size_t)v * ROW);
-      uint4* dst = reinterpret_cast<uint4*>(qs.snap + ((size_t)(qs.snap_h - 1u) * qs.nv + v) * ROW);
-      const uint4 a = __ldcg(src), b = __ldcg(src + 1);
-      dst[0] = a;
-      dst[1] = b;
-      if (qs.snap_h == qs.star_h || qs.snap_h == qs.center_h) {
-        // the rows are the exact distances over paths of at most snap_h hops
-        const uint32_t r[KMAX] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z};
-        bool all = true;
-        unsigned long long sum = 0;
-#pragma unroll
-        for (int t = 0; t < KMAX; t++)
-          if (t < qs.k) {
-            all = all && r[t] != INF32;
-            sum += r[t];
-          }
-        if (all && qs.snap_h == qs.center_h && __ldca(&qs.ctl->center) == 0u) atomicExch(&qs.ctl->center, 1u);
-        // v joined to every group by its cheapest path of at most star_h
-        // hops: a breadth-first tree from v inside their union has depth <=
-        // star_h, so diameter <= 2 * star_h <= D, at cost <= sum
-        if (all && qs.snap_h == qs.star_h && sum < ld_best(qs.ctl)) atomicMin(&qs.ctl->best, (uint32_t)sum);
-      }
-    }
+    if (task < nbig)
+      chunk_task(qd, rd, g, task, lane, &s_hub[threadIdx.x >> 5], ws, wb);
+    else
+      heavy_static_task(qd, pre, s_lb, nslots, task - nbig, snap0, n_lb, n_snap, lane, s_dl[threadIdx.x >> 5]);
   }
   wb_flush(wb, lane);
   if (lane == 0) ws_flush(ws);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent round loop: R rounds in one cooperative launch (every block
+// resident at once).  Block 0 runs the first control step; the last block to
+// finish a round's work runs the next one.  A round is
+//   wait for its control step (epoch) -> light tasks and the static heavy
+//   tasks (bound rows, snapshots), taken by warp striding -> every block done
+//   with those (phase1: the arc chunks the light tasks handed over are all
+//   written) -> the chunks -> arrive; the last block to arrive runs the next
+//   control step and publishes it.
+// Every wait is bounded by pc->timeout_ns (and an iteration limit): when one
+// expires the launch sets pc->err and every block returns, the host fails
+// the admitted queries with GST_DEVICE_TIMEOUT and the context stays usable.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// One thread: wait until *flag >= target.  False when the launch has failed
+// (another wait expired) or this one expires.
+__device__ bool wait_geq(const uint32_t* flag, uint32_t target, PersistCtl* pc, uint32_t where) {
+  const unsigned long long t0 = global_ns(), lim = pc->timeout_ns;
+  uint32_t ns = 32;
+  for (uint32_t it = 0; it < (1u << 25); it++) {
+    if (ld_acquire_gpu(flag) >= target) return true;
+    if (ld_acquire_gpu(&pc->err)) return false;
+    if (global_ns() - t0 > lim) break;
+    __nanosleep(ns);
+    if (ns < 1024u) ns <<= 1;
+  }
+  atomicCAS(&pc->err_where, 0u, where);
+  atomicExch(&pc->err, 1u);
+  return false;
+}
+
+// Publish control step `e` (after its writes).  One thread.
+__device__ __forceinline__ void publish(PersistCtl* pc, uint32_t e) {
+  __threadfence();
+  if (!pc->hold) st_release_gpu(&pc->epoch, e);
+}
+
+struct RoundSmem {
+  uint32_t pre_sssp[MAX_SLOTS + 1], pre_dp[MAX_SLOTS + 1], pre_hop[MAX_SLOTS + 1], pre_lb[MAX_SLOTS + 1];
+  WarpScratch w[8];
+  WarpStat ws[8];
+  WarpBuf wb[8];
+  CtlSmem ctl;
+  uint32_t ok, last;
+};
+
+__global__ void __launch_bounds__(256, 3) k_rounds(QDev* qd, QCtl* ctl, int nslots_ctl, RoundDesc* rd, uint32_t* pre,
+                                                GraphDev g, uint32_t R, PersistCtl* pc) {
+  __shared__ RoundSmem sm;
+  const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+  const uint32_t warp = blockIdx.x * (blockDim.x >> 5) + wib;
+  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+  WarpStat& ws = sm.ws[wib];
+  WarpBuf& wb = sm.wb[wib];
+  if (blockIdx.x == 0) {
+    control_step(qd, ctl, nslots_ctl, rd, pre, sm.ctl);
+    __syncthreads();
+    if (threadIdx.x == 0) publish(pc, 1u);
+  }
+  for (uint32_t r = 0; r < R; r++) {
+    if (threadIdx.x == 0) {
+      sm.ok = wait_geq(&pc->epoch, r + 1u, pc, 1u) ? 1u : 0u;
+      __threadfence();
+    }
+    __syncthreads();
+    if (!sm.ok) return;
+    // a round with no live query does nothing, nor do the rest: every block
+    // reads the same count, so every block leaves here together
+    if (__ldcg(&rd->n_live) == 0u) return;
+    const int nslots = min(nslots_ctl, (int)__ldcg(&rd->nslots));
+    for (int i = threadIdx.x; i <= nslots; i += blockDim.x) {
+      sm.pre_sssp[i] = __ldcg(pre + T_SSSP * (MAX_SLOTS + 1) + i);
+      sm.pre_dp[i] = __ldcg(pre + T_DP * (MAX_SLOTS + 1) + i);
+      sm.pre_hop[i] = __ldcg(pre + T_HOP * (MAX_SLOTS + 1) + i);
+      sm.pre_lb[i] = __ldcg(pre + T_LB * (MAX_SLOTS + 1) + i);
+    }
+    if (lane == 0) {
+      ws_init(ws);
+      wb_init(wb);
+    }
+    __syncthreads();
+    const uint32_t ntl = __ldcg(&rd->light_tasks), nth = __ldcg(&rd->heavy_tasks);
+    const uint32_t n_lb = __ldcg(&rd->items[T_LB]), n_snap = __ldcg(&rd->items[T_SNAP]);
+    const uint32_t snap0 = __ldcg(&rd->task_off[T_SNAP]);
+    for (uint32_t task = warp; task < ntl; task += nwarps)
+      light_task(qd, rd, pre, sm.pre_sssp, sm.pre_dp, sm.pre_hop, nslots, g, task, lane, ws, wb, sm.w[wib]);
+    for (uint32_t ht = warp; ht < nth; ht += nwarps)
+      heavy_static_task(qd, pre, sm.pre_lb, nslots, ht, snap0, n_lb, n_snap, lane, sm.w[wib].dl);
+    // phase 1 done in this block: its chunk entries are written
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(&pc->phase1, 1u);
+      sm.ok = wait_geq(&pc->phase1, (r + 1u) * gridDim.x, pc, 2u) ? 1u : 0u;
+      __threadfence();
+    }
+    __syncthreads();
+    if (sm.ok) {
+      const uint32_t nbig = rd->big ? min(__ldcg(&rd->n_big), rd->big_cap) : 0u;
+      for (uint32_t i = warp; i < nbig; i += nwarps) chunk_task(qd, rd, g, i, lane, &sm.w[wib].hdr[0], ws, wb);
+    }
+    wb_flush(wb, lane);
+    if (lane == 0) ws_flush(ws);
+    __syncthreads();
+    if (!sm.ok) return;
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const uint32_t old = atomicAdd(&pc->arrive, 1u);
+      sm.last = old == (r + 1u) * gridDim.x - 1u ? 1u : 0u;
+      if (sm.last) {
+        __threadfence();  // every block's round work is visible from here on
+        pc->rounds = r + 1u;
+      }
+    }
+    __syncthreads();
+    if (sm.last && r + 1u < R) {
+      control_step(qd, ctl, nslots_ctl, rd, pre, sm.ctl);
+      __syncthreads();
+      if (threadIdx.x == 0) publish(pc, r + 2u);
+    }
+    __syncthreads();  // sm.ok and sm.last are rewritten next round
+  }
 }
 
 }  // namespace gstb

@@ -45,9 +45,15 @@ class GstError(RuntimeError):
         super().__init__(f"{what}: {STATUS_NAMES.get(status, status)}{detail}")
 
 
+TUNING_FIELDS = ("delta_sssp", "delta_dp", "hub_min_deg", "cap_pct", "persistent", "rounds_per_launch",
+                 "dp_wmax", "sssp_wmax", "merge_stage")
+
+
 class _Tuning(ctypes.Structure):
-    _fields_ = [("delta_sssp", ctypes.c_uint32), ("delta_dp", ctypes.c_uint32), ("hub_min_deg", ctypes.c_uint32),
-                ("cap_pct", ctypes.c_uint32)]
+    _fields_ = [(n, ctypes.c_uint32) for n in TUNING_FIELDS]
+
+    def as_dict(self) -> dict:
+        return {n: int(getattr(self, n)) for n in TUNING_FIELDS}
 
 
 class _ServeInfo(ctypes.Structure):
@@ -111,8 +117,9 @@ def lib():
         L.gst_serve_set_max_pending.argtypes = [vp, u64]
         L.gst_serve_stats.argtypes = [vp, ctypes.POINTER(_ServeInfo)]
         L.gst_debug_fail_allocs.argtypes = [vp, ctypes.c_int]
+        L.gst_debug_hold_rounds.argtypes = [vp, ctypes.c_int, ctypes.c_uint32]
         for name in ("gst_serve_open", "gst_serve_submit", "gst_serve_poll", "gst_serve_close", "gst_serve_cancel",
-                     "gst_serve_set_max_pending", "gst_serve_stats", "gst_debug_fail_allocs"):
+                     "gst_serve_set_max_pending", "gst_serve_stats", "gst_debug_fail_allocs", "gst_debug_hold_rounds"):
             getattr(L, name).restype = ctypes.c_int
         for name in ("gst_graph_create", "gst_groups_set", "gst_query", "gst_query_batch", "gst_query_batch_ratio",
                      "gst_query_ratio", "gst_serve_submit_ratio"):
@@ -194,6 +201,14 @@ class Engine:
         if st != GST_OK:
             raise GstError(st, "gst_debug_fail_allocs")
 
+    def hold_rounds(self, hold: bool, timeout_ms: int = 0):
+        """Test hook (gst_debug_hold_rounds): while held, persistent round
+        launches publish no control step, so their bounded waits expire after
+        timeout_ms and the admitted queries end with GST_DEVICE_TIMEOUT."""
+        st = lib().gst_debug_hold_rounds(self._h, 1 if hold else 0, int(timeout_ms))
+        if st != GST_OK:
+            raise GstError(st, "gst_debug_hold_rounds")
+
     def kernel_launches(self) -> int:
         return int(lib().gst_kernel_launches(self._h))
 
@@ -217,14 +232,16 @@ class Engine:
         st = lib().gst_tuning_get(self._h, ctypes.byref(t))
         if st != GST_OK:
             raise GstError(st, "gst_tuning_get")
-        return {"delta_sssp": t.delta_sssp, "delta_dp": t.delta_dp, "hub_min_deg": t.hub_min_deg,
-                "cap_pct": t.cap_pct}
+        return t.as_dict()
 
     def set_tuning(self, **kw):
         """Change launch parameters (gst_tuning_set); unnamed ones keep their values."""
         cur = self.tuning()
+        unknown = set(kw) - set(TUNING_FIELDS)
+        if unknown:
+            raise ValueError(f"unknown launch parameters {sorted(unknown)}")
         cur.update(kw)
-        t = _Tuning(cur["delta_sssp"], cur["delta_dp"], cur["hub_min_deg"], cur["cap_pct"])
+        t = _Tuning(*[cur[n] for n in TUNING_FIELDS])
         st = lib().gst_tuning_set(self._h, ctypes.byref(t))
         if st != GST_OK:
             raise GstError(st, "gst_tuning_set")
@@ -244,8 +261,7 @@ class Engine:
                                 0 if objective == "throughput" else 1, ctypes.byref(t))
         if st != GST_OK:
             raise GstError(st, "gst_autotune")
-        return {"delta_sssp": t.delta_sssp, "delta_dp": t.delta_dp, "hub_min_deg": t.hub_min_deg,
-                "cap_pct": t.cap_pct}
+        return t.as_dict()
 
     def query(self, groups, D: int = -1, max_edges: int = 4096, ratio: float = 0.0) -> QueryResult:
         """One synchronous query (gst_query; gst_query_ratio when ratio > 1:

@@ -164,21 +164,33 @@ gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, int k, int D,
  * reference fixes its block sizes and thresholds at compile time, DPQ.cuh:43
  * and GPUGST+/include/util.h:19-33).  Defaults, overridable at
  * gst_graph_create by GSTB_DELTA_SSSP / GSTB_DELTA_DP / GSTB_HUB_MIN_DEG /
- * GSTB_SSSP_CAP_PCT: 16, 8, 256, 60.  None of them changes a result, only the
- * work schedule and how tight the lower bounds are. */
+ * GSTB_SSSP_CAP_PCT / GSTB_PERSIST / GSTB_ROUNDS_PER_SYNC / GSTB_DP_WMAX /
+ * GSTB_SSSP_WMAX / GSTB_MERGE_STAGE: 16, 8, 256, 60, 0, 4, 32, 32, 0.  None
+ * of them changes a result, only the work schedule and how tight the lower
+ * bounds are. */
 typedef struct gst_tuning {
   uint32_t delta_sssp;   /* width of the distance rounds' near-far window */
   uint32_t delta_dp;     /* width of the DP rounds' near-far window */
   uint32_t hub_min_deg;  /* a vertex with this many arcs to relax hands them out in chunks (>= 32) */
   uint32_t cap_pct;      /* distances are computed exactly up to this percentage of the incumbent (1..100) */
+  uint32_t persistent;   /* 1: each block of rounds is one persistent cooperative launch (the round
+                            loop runs on the device, every block resident); 0: a CUDA graph of
+                            control / light / heavy launches per round */
+  uint32_t rounds_per_launch; /* rounds per block (1..64); between blocks the host retires finished
+                                 queries and admits new ones */
+  uint32_t dp_wmax;      /* most DP states per warp task: 1, 2, 4, 8, 16 or 32 */
+  uint32_t sssp_wmax;    /* most distance items (vertices) per warp task: 4, 8, 16 or 32 */
+  uint32_t merge_stage;  /* merge tile: a DP state with at least this many merge partners first
+                            stages its vertex's table and bound rows in shared memory (0: never) */
 } gst_tuning;
 
 gst_status gst_tuning_get(gst_graph* g, gst_tuning* out);
 gst_status gst_tuning_set(gst_graph* g, const gst_tuning* t);
 /* Autotuner for the graph's degree profile: times a sample of n queries
  * (laid out as for gst_query_batch) under candidate settings (cap_pct 50/60/
- * 67/75, delta_sssp 8..64, delta_dp 2..16, hub_min_deg 128..1024), one
- * parameter at a time, and keeps the fastest.  objective 0 = batch throughput
+ * 67/75, delta_sssp 8..64, delta_dp 2..16, hub_min_deg 128..1024, persistent
+ * 0/1, rounds_per_launch 2..16, dp_wmax 4..32, sssp_wmax 8..32, merge_stage
+ * 0/6/14/30), one parameter at a time, and keeps the fastest.  objective 0 = batch throughput
  * (gst_query_batch), 1 = one query at a time (gst_query).  The chosen
  * settings stay on the graph; out (may be null) receives them. */
 gst_status gst_autotune(gst_graph* g, int n, const uint32_t* groups, const int32_t* ks, const int32_t* Ds,
@@ -251,6 +263,12 @@ gst_status gst_serve_close(gst_server* s);
  * query that cannot be admitted while nothing else runs returns GST_OOM;
  * with others running it waits for their memory. */
 gst_status gst_debug_fail_allocs(gst_graph* g, int n);
+/* Test hook for the persistent round launch's bounded waits: while hold is 1
+ * its control steps are not published, so every wait of a launch expires
+ * after timeout_ms (0: the default, GSTB_WAIT_MS or 30000) and the admitted
+ * queries end with GST_DEVICE_TIMEOUT; the device stays usable.  hold 0 and
+ * timeout_ms 0 restore normal running. */
+gst_status gst_debug_hold_rounds(gst_graph* g, int hold, uint32_t timeout_ms);
 
 const char* gst_status_string(gst_status st);
 /* The CUDA runtime's description of the last CUDA error any gstb call in this
@@ -259,9 +277,11 @@ const char* gst_last_cuda_error(void);
 
 /* Diagnostics (no reference counterpart).  Kernel launches issued by this
  * graph's engine so far, and, when profiling is on (gst_query_batch calls
- * only), the accumulated device time of the two round kernels
+ * only), the accumulated device time of the round kernels
  * (kernel_ms[0] = k_light: distance items, splits, seeds, tours,
- * extraction; kernel_ms[1] = k_heavy: lower-bound rows and DP states), the
+ * extraction, DP states; kernel_ms[1] = k_heavy: arc chunks, lower-bound
+ * rows, snapshots; when the rounds ran as persistent launches,
+ * kernel_ms[0] = k_rounds, all of the round, and kernel_ms[1] = 0), the
  * number of rounds, and the summed GST_STAT_* counters of finished queries. */
 uint64_t gst_kernel_launches(const gst_graph* g);
 void gst_profile_enable(gst_graph* g, int on);
