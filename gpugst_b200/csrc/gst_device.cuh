@@ -79,11 +79,13 @@ struct RoundDesc {
 };
 // State of one persistent round launch (k_rounds), written by the host
 // before each launch (the counters zero).
+// The polled word and the two arrival counters sit in cache lines of their
+// own, so that polling blocks do not queue on the counters' atomics.
 struct PersistCtl {
-  uint32_t epoch;    // control steps published (round r's work waits for epoch >= r + 1)
-  uint32_t arrive;   // blocks that finished their round work, summed over rounds
-  uint32_t phase1;   // blocks that finished the light and static heavy tasks, summed over rounds
-  uint32_t err;      // 1: a bounded wait expired, the launch stopped
+  alignas(128) uint32_t epoch;  // control steps published (round r's work waits for epoch >= r + 1)
+  alignas(128) uint32_t arrive; // blocks that finished their round work, summed over rounds
+  alignas(128) uint32_t phase1; // blocks done with the light and static heavy tasks, summed over chunk rounds
+  alignas(128) uint32_t err;    // 1: a bounded wait expired, the launch stopped
   uint32_t err_where;  // the first wait that expired: 1 control step, 2 light tasks
   uint32_t rounds;   // rounds completed
   uint32_t hold;     // 1: control steps are not published (makes the waits expire; a test of them)

@@ -864,7 +864,9 @@ class Runner {
       tp.hold = g_->hold_rounds.load();
       CK(cudaMemcpyAsync(d_pc_, &tp, sizeof(PersistCtl), cudaMemcpyHostToDevice, stream_));
       GraphDev gd{g_->d_beg, g_->d_adj, g_->V, g_->d_wcut};
-      int nsc = (int)max_slots_;
+      // the control steps scan the slots in use: admissions happen only
+      // between launches, so none above the highest one starts during it
+      int nsc = (int)std::max<uint32_t>(1u, nslots_hi_);
       uint32_t R32 = R;
       PersistCtl* pc = d_pc_;
       void* args[] = {&d_qd_, &d_ctl_, &nsc, &d_rd_, &d_pre_, &gd, &R32, &pc};
@@ -1193,7 +1195,7 @@ gst_status gst_graph_create(const uint32_t* beg_pos, const uint32_t* csr, const 
   g->tune.rounds_per_launch = std::min(64u, std::max(1u, env_u32("GSTB_ROUNDS_PER_SYNC", 4)));
   g->tune.dp_wmax = floor_pow2(std::min(32u, std::max(1u, env_u32("GSTB_DP_WMAX", 32))));
   g->tune.sssp_wmax = floor_pow2(std::min(32u, std::max(4u, env_u32("GSTB_SSSP_WMAX", 32))));
-  g->tune.merge_stage = env_u32("GSTB_MERGE_STAGE", 0);
+  g->tune.merge_stage = env_u32("GSTB_MERGE_STAGE", 14);
   cudaGetDevice(&g->device);
   cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device);
   {

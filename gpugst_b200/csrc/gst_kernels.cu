@@ -1966,15 +1966,19 @@ __global__ void __launch_bounds__(256, 3) k_heavy(const QDev* __restrict__ qd, R
 //   wait for its control step (epoch) -> light tasks and the static heavy
 //   tasks (bound rows, snapshots), taken by warp striding -> every block done
 //   with those (phase1: the arc chunks the light tasks handed over are all
-//   written) -> the chunks -> arrive; the last block to arrive runs the next
-//   control step and publishes it.
+//   written; skipped in rounds that hand out none) -> the chunks -> arrive;
+//   the last block to arrive runs the next control step and publishes it.
 // Every wait is bounded by pc->timeout_ns (and an iteration limit): when one
 // expires the launch sets pc->err and every block returns, the host fails
 // the admitted queries with GST_DEVICE_TIMEOUT and the context stays usable.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+// The waits poll with relaxed loads (read at L2, leaving the SM's L1 alone)
+// and order what follows with one fence once the flag is seen: an acquire at
+// every poll would invalidate the L1 of an SM whose other blocks are still
+// working from it.
+__device__ __forceinline__ uint32_t ld_relaxed_gpu(const uint32_t* p) {
   uint32_t v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
 __device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
@@ -1986,14 +1990,17 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// One thread: wait until *flag >= target.  False when the launch has failed
-// (another wait expired) or this one expires.
+// One thread: wait until *flag >= target, then fence (the acquire).  False
+// when the launch has failed (another wait expired) or this one expires.
 __device__ bool wait_geq(const uint32_t* flag, uint32_t target, PersistCtl* pc, uint32_t where) {
   const unsigned long long t0 = global_ns(), lim = pc->timeout_ns;
   uint32_t ns = 32;
   for (uint32_t it = 0; it < (1u << 25); it++) {
-    if (ld_acquire_gpu(flag) >= target) return true;
-    if (ld_acquire_gpu(&pc->err)) return false;
+    if (ld_relaxed_gpu(flag) >= target) {
+      __threadfence();
+      return true;
+    }
+    if (ld_relaxed_gpu(&pc->err)) return false;
     if (global_ns() - t0 > lim) break;
     __nanosleep(ns);
     if (ns < 1024u) ns <<= 1;
@@ -2026,16 +2033,14 @@ __global__ void __launch_bounds__(256, 3) k_rounds(QDev* qd, QCtl* ctl, int nslo
   const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
   WarpStat& ws = sm.ws[wib];
   WarpBuf& wb = sm.wb[wib];
+  uint32_t p1 = 0;  // rounds with a chunk phase so far (the same in every block)
   if (blockIdx.x == 0) {
     control_step(qd, ctl, nslots_ctl, rd, pre, sm.ctl);
     __syncthreads();
     if (threadIdx.x == 0) publish(pc, 1u);
   }
   for (uint32_t r = 0; r < R; r++) {
-    if (threadIdx.x == 0) {
-      sm.ok = wait_geq(&pc->epoch, r + 1u, pc, 1u) ? 1u : 0u;
-      __threadfence();
-    }
+    if (threadIdx.x == 0) sm.ok = wait_geq(&pc->epoch, r + 1u, pc, 1u) ? 1u : 0u;
     __syncthreads();
     if (!sm.ok) return;
     // a round with no live query does nothing, nor do the rest: every block
@@ -2060,13 +2065,17 @@ __global__ void __launch_bounds__(256, 3) k_rounds(QDev* qd, QCtl* ctl, int nslo
       light_task(qd, rd, pre, sm.pre_sssp, sm.pre_dp, sm.pre_hop, nslots, g, task, lane, ws, wb, sm.w[wib]);
     for (uint32_t ht = warp; ht < nth; ht += nwarps)
       heavy_static_task(qd, pre, sm.pre_lb, nslots, ht, snap0, n_lb, n_snap, lane, sm.w[wib].dl);
-    // phase 1 done in this block: its chunk entries are written
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      __threadfence();
-      atomicAdd(&pc->phase1, 1u);
-      sm.ok = wait_geq(&pc->phase1, (r + 1u) * gridDim.x, pc, 2u) ? 1u : 0u;
-      __threadfence();
+    // phase 1 done in this block: its chunk entries are written.  Rounds
+    // that hand out no chunks (every block reads the same flags) skip the
+    // grid-wide wait for the others
+    if (rd->big != nullptr && (__ldcg(&rd->hub_on) | __ldcg(&rd->grow_chunks))) {
+      p1++;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&pc->phase1, 1u);
+        sm.ok = wait_geq(&pc->phase1, p1 * gridDim.x, pc, 2u) ? 1u : 0u;
+      }
     }
     __syncthreads();
     if (sm.ok) {

@@ -165,7 +165,7 @@ gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, int k, int D,
  * and GPUGST+/include/util.h:19-33).  Defaults, overridable at
  * gst_graph_create by GSTB_DELTA_SSSP / GSTB_DELTA_DP / GSTB_HUB_MIN_DEG /
  * GSTB_SSSP_CAP_PCT / GSTB_PERSIST / GSTB_ROUNDS_PER_SYNC / GSTB_DP_WMAX /
- * GSTB_SSSP_WMAX / GSTB_MERGE_STAGE: 16, 8, 256, 60, 0, 4, 32, 32, 0.  None
+ * GSTB_SSSP_WMAX / GSTB_MERGE_STAGE: 16, 8, 256, 60, 0, 4, 32, 32, 14.  None
  * of them changes a result, only the work schedule and how tight the lower
  * bounds are. */
 typedef struct gst_tuning {
