@@ -2002,8 +2002,10 @@ __device__ bool wait_geq(const uint32_t* flag, uint32_t target, PersistCtl* pc, 
     }
     if (ld_relaxed_gpu(&pc->err)) return false;
     if (global_ns() - t0 > lim) break;
-    __nanosleep(ns);
-    if (ns < 1024u) ns <<= 1;
+    if (it >= 64u) {  // a short wait polls back to back, a long one backs off to 1 us
+      __nanosleep(ns);
+      if (ns < 1024u) ns <<= 1;
+    }
   }
   atomicCAS(&pc->err_where, 0u, where);
   atomicExch(&pc->err, 1u);
@@ -2061,10 +2063,15 @@ __global__ void __launch_bounds__(256, 3) k_rounds(QDev* qd, QCtl* ctl, int nslo
     const uint32_t ntl = __ldcg(&rd->light_tasks), nth = __ldcg(&rd->heavy_tasks);
     const uint32_t n_lb = __ldcg(&rd->items[T_LB]), n_snap = __ldcg(&rd->items[T_SNAP]);
     const uint32_t snap0 = __ldcg(&rd->task_off[T_SNAP]);
-    for (uint32_t task = warp; task < ntl; task += nwarps)
-      light_task(qd, rd, pre, sm.pre_sssp, sm.pre_dp, sm.pre_hop, nslots, g, task, lane, ws, wb, sm.w[wib]);
-    for (uint32_t ht = warp; ht < nth; ht += nwarps)
-      heavy_static_task(qd, pre, sm.pre_lb, nslots, ht, snap0, n_lb, n_snap, lane, sm.w[wib].dl);
+    // light tasks, then the static heavy ones, as one list dealt out over
+    // the warps (two lists dealt out one after the other would leave the
+    // warps with the heaviest light tasks also the first heavy ones)
+    for (uint32_t task = warp; task < ntl + nth; task += nwarps) {
+      if (task < ntl)
+        light_task(qd, rd, pre, sm.pre_sssp, sm.pre_dp, sm.pre_hop, nslots, g, task, lane, ws, wb, sm.w[wib]);
+      else
+        heavy_static_task(qd, pre, sm.pre_lb, nslots, task - ntl, snap0, n_lb, n_snap, lane, sm.w[wib].dl);
+    }
     // phase 1 done in this block: its chunk entries are written.  Rounds
     // that hand out no chunks (every block reads the same flags) skip the
     // grid-wide wait for the others
