@@ -426,6 +426,9 @@ def main():
     ap.add_argument("--c5-max-pending", type=int, default=256)
     ap.add_argument("--c5-drain", type=float, default=5.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--modes", type=int, default=1,
+                    help="compare the two round-launch modes (CUDA-graph blocks, persistent launches) on rank 0")
+    ap.add_argument("--modes-plain", type=int, default=60, help="plain queries per launch mode")
     ap.add_argument("--c2-sweep", type=int, default=1,
                     help="with the batched configuration, also run the plain path and the serving sweep on the "
                          "170k-vertex workload (0: off)")
@@ -534,10 +537,41 @@ def main():
     dp_bytes = dp_work_bytes(st, lb_rows)
     peak, peak_kind = measured_peak_hbm()
     round_ms = light_ms + heavy_ms
+    if E.tuning()["persistent"]:  # the rounds ran as persistent launches: one kernel
+        rkernel, kernel_ms = "round (k_rounds, persistent)", {"k_rounds": light_ms}
+    else:
+        rkernel, kernel_ms = "round (k_light + k_heavy)", {"k_light": light_ms, "k_heavy": heavy_ms}
     round_bytes = dist_bytes + dp_bytes
     achieved = round_bytes / (round_ms / 1e3) / 1e9 if round_ms > 0 else 0.0
     tpb = traffic_per_byte()
     per_round_alg = round_bytes / max(prof_rounds, 1)
+
+    # the two round-launch modes on the same batches and plain queries
+    # (device time): blocks of control / light / heavy launches as CUDA
+    # graphs, and persistent cooperative launches (k_rounds)
+    modes = None
+    if rank == 0 and args.modes:
+        modes = {}
+        keep = E.tuning()
+        for name, pv in (("graph", 0), ("persistent", 1)):
+            E.set_tuning(persistent=pv)
+            E.query_batch(*batch_for(1))
+            dms, nb = 0.0, 0
+            for s in range(2):
+                r = E.query_batch(*batch_for(2 + s))
+                dms += r[0].device_ms
+                nb += len(r)
+            pl, pd = [], []
+            for i in range(args.modes_plain):
+                j = (i * 37) % nq_set
+                t0 = time.perf_counter()
+                rp = E.query(qs[j], D=Ds[j])
+                pl.append(1e3 * (time.perf_counter() - t0))
+                pd.append(rp.device_ms)
+            modes[name] = {"batched_qps_device": nb / (dms / 1e3), "batched_queries": nb,
+                           "plain_ms_mean": sum(pl) / len(pl), "plain_ms_p50": pct(pl, 50),
+                           "plain_device_ms_mean": sum(pd) / len(pd), "plain_queries": len(pl)}
+        E.set_tuning(**keep)
 
     # plain per-query path (one query per call, gst_query), same query set
     plain_lat, plain_dev = [], []
@@ -626,11 +660,12 @@ def main():
             "serve_vs_plain_best": best_pt["vs_plain"] if best_pt else None,
             "open_loop": c5,
             "c2_170k": c2,
-            "roofline": {"bound": "hbm", "kernel": "round (k_light + k_heavy)", "achieved": achieved,
+            "launch_modes": modes,
+            "roofline": {"bound": "hbm", "kernel": rkernel, "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": (per_round_alg * tpb) if tpb else None,
                          "algorithmic_bytes_per_round": per_round_alg, "rounds": prof_rounds,
-                         "kernel_ms": {"k_light": light_ms, "k_heavy": heavy_ms},
+                         "kernel_ms": kernel_ms,
                          "algorithmic_bytes": {"distance": dist_bytes, "dp": dp_bytes}},
             "cpu_baseline": cpu,
             "clocks": clocks,
