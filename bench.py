@@ -427,7 +427,8 @@ def main():
     ap.add_argument("--c5-drain", type=float, default=5.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--modes", type=int, default=1,
-                    help="compare the two round-launch modes (CUDA-graph blocks, persistent launches) on rank 0")
+                    help="compare the round-launch modes (CUDA-graph blocks, persistent launches, 128-thread "
+                         "blocks) on rank 0")
     ap.add_argument("--modes-plain", type=int, default=60, help="plain queries per launch mode")
     ap.add_argument("--c2-sweep", type=int, default=1,
                     help="with the batched configuration, also run the plain path and the serving sweep on the "
@@ -546,15 +547,16 @@ def main():
     tpb = traffic_per_byte()
     per_round_alg = round_bytes / max(prof_rounds, 1)
 
-    # the two round-launch modes on the same batches and plain queries
-    # (device time): blocks of control / light / heavy launches as CUDA
-    # graphs, and persistent cooperative launches (k_rounds)
+    # the round-launch modes on the same batches and plain queries (device
+    # time): blocks of control / light / heavy launches as CUDA graphs, and
+    # persistent cooperative launches (k_rounds), at 256 threads a block; and
+    # the graph blocks at 128
     modes = None
     if rank == 0 and args.modes:
         modes = {}
         keep = E.tuning()
-        for name, pv in (("graph", 0), ("persistent", 1)):
-            E.set_tuning(persistent=pv)
+        for name, pv, bt in (("graph", 0, 256), ("persistent", 1, 256), ("graph_128_threads", 0, 128)):
+            E.set_tuning(persistent=pv, block_threads=bt)
             E.query_batch(*batch_for(1))
             dms, nb = 0.0, 0
             for s in range(2):

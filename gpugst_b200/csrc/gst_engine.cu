@@ -35,10 +35,11 @@
 
 namespace gstb {
 __global__ void k_control(QDev*, QCtl*, int, RoundDesc*, uint32_t*);
-__global__ void k_light(const QDev*, RoundDesc*, const uint32_t*, int, GraphDev);
-__global__ void k_heavy(const QDev*, RoundDesc*, const uint32_t*, int, GraphDev);
+// the round kernels of a block size (128 or 256 threads; null otherwise)
+const void* light_kernel(int threads);
+const void* heavy_kernel(int threads);
+const void* rounds_kernel(int threads);
 __global__ void k_init_workspace(uint4*, size_t, uint4*, uint4*, uint32_t, uint4*, size_t);
-__global__ void k_rounds(QDev*, QCtl*, int, RoundDesc*, uint32_t*, GraphDev, uint32_t, PersistCtl*);
 }  // namespace gstb
 
 using namespace gstb;
@@ -427,25 +428,8 @@ class Runner {
     CK(cudaMalloc(&d_ctl_, MAX_SLOTS * sizeof(QCtl)));
     CK(cudaMalloc(&d_rd_, sizeof(RoundDesc)));
     {
-      // grids: every SM filled to the occupancy limit of each kernel
-      int bl = 0, bh = 0;
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, k_light, 256, 0));
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bh, k_heavy, 256, 0));
-      light_grid_ = (unsigned)g_->num_sms * (unsigned)std::max(1, bl);
-      heavy_grid_ = (unsigned)g_->num_sms * (unsigned)std::max(1, bh);
-      resident_light_warps_ = light_grid_ * (256 / 32);
-      // GSTB_GRID_WAVES > 1 launches that many resident waves of blocks: a
-      // block that runs out of tasks early exits and a waiting block takes
-      // its place on the SM
-      const unsigned waves = std::min(8u, std::max(1u, env_u32("GSTB_GRID_WAVES", 1)));
-      light_grid_ *= waves;
-      heavy_grid_ *= waves;
-      // the persistent round launch: one resident wave, every block at once
-      int br = 0, coop = 0;
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&br, k_rounds, 256, 0));
-      CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, g_->device));
-      rounds_grid_ = coop ? (unsigned)g_->num_sms * (unsigned)std::max(0, br) : 0u;
-      persist_ = rounds_grid_ > 0 && g_->tune.persistent;
+      gst_status gs = setup_grids();
+      if (gs != GST_OK) return gs;
     }
     {
       // hub arc chunk list (k_light -> k_heavy within a round)
@@ -459,7 +443,7 @@ class Runner {
       rd.hub_min_rest = env_u32("GSTB_HUB_MIN_REST", 128);
       rd.hub_max_items = env_u32("GSTB_HUB_MAX_ITEMS", 1000000);
       // task widths are sized for the warps resident at once
-      rd.light_warps = persist_ ? rounds_grid_ * (256 / 32) : resident_light_warps_;
+      rd.light_warps = light_warps();
       rd.sssp_w = 4;
       rd.dp_wmax = g_->tune.dp_wmax;
       rd.sssp_wmax = g_->tune.sssp_wmax;
@@ -492,6 +476,51 @@ class Runner {
       if (gs != GST_OK) return gs;
     }
     return GST_OK;
+  }
+
+  // Grids of the round kernels for the graph's block size: every SM filled
+  // to the occupancy limit of each kernel.
+  gst_status setup_grids() {
+    const int T = (int)g_->tune.block_threads;
+    kl_ = light_kernel(T);
+    kh_ = heavy_kernel(T);
+    kr_ = rounds_kernel(T);
+    if (!kl_ || !kh_ || !kr_) return GST_BAD_INPUT;
+    threads_ = (uint32_t)T;
+    int bl = 0, bh = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, kl_, T, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bh, kh_, T, 0));
+    light_grid_ = (unsigned)g_->num_sms * (unsigned)std::max(1, bl);
+    heavy_grid_ = (unsigned)g_->num_sms * (unsigned)std::max(1, bh);
+    resident_light_warps_ = light_grid_ * ((unsigned)T / 32);
+    // GSTB_GRID_WAVES > 1 launches that many resident waves of blocks: a
+    // block that runs out of tasks early exits and a waiting block takes
+    // its place on the SM
+    const unsigned waves = std::min(8u, std::max(1u, env_u32("GSTB_GRID_WAVES", 1)));
+    light_grid_ *= waves;
+    heavy_grid_ *= waves;
+    // the persistent round launch: one resident wave, every block at once
+    int br = 0, coop = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&br, kr_, T, 0));
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, g_->device));
+    rounds_grid_ = coop ? (unsigned)g_->num_sms * (unsigned)std::max(0, br) : 0u;
+    persist_ = rounds_grid_ > 0 && g_->tune.persistent;
+    return GST_OK;
+  }
+
+  // Warps of one round launch: the task widths are sized for them.
+  uint32_t light_warps() const { return persist_ ? rounds_grid_ * (threads_ / 32) : resident_light_warps_; }
+
+  // k_light / k_heavy of the graph's block size on the runner's stream.
+  cudaError_t launch_light(const GraphDev& gd, int ns) {
+    GraphDev g = gd;
+    void* args[] = {&d_qd_, &d_rd_, &d_pre_, &ns, &g};
+    return cudaLaunchKernel(kl_, dim3(light_grid_), dim3(threads_), args, 0, stream_);
+  }
+  cudaError_t launch_heavy(const GraphDev& gd, int ns) {
+    GraphDev g = gd;
+    void* args[] = {&d_qd_, &d_rd_, &d_pre_, &ns, &g};
+    return cudaLaunchKernel(kh_, dim3(heavy_grid_), dim3(threads_), args, 0, stream_);
   }
 
   void release() {
@@ -584,15 +613,20 @@ class Runner {
     cap_den_ = 100;
     const uint32_t hub = g_->tune.hub_min_deg, dpw = g_->tune.dp_wmax, ssw = g_->tune.sssp_wmax;
     const uint32_t mst = g_->tune.merge_stage;
+    const bool regrid = g_->tune.block_threads != threads_;
+    if (regrid) {
+      gst_status gs = setup_grids();
+      if (gs != GST_OK) return gs;
+    }
     persist_ = rounds_grid_ > 0 && g_->tune.persistent;
-    const uint32_t lw = persist_ ? rounds_grid_ * (256 / 32) : resident_light_warps_;
+    const uint32_t lw = light_warps();
     CK(cudaMemcpyAsync(&d_rd_->hub_min_deg, &hub, sizeof(hub), cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(&d_rd_->dp_wmax, &dpw, sizeof(dpw), cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(&d_rd_->sssp_wmax, &ssw, sizeof(ssw), cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(&d_rd_->merge_stage, &mst, sizeof(mst), cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(&d_rd_->light_warps, &lw, sizeof(lw), cudaMemcpyHostToDevice, stream_));
     CK(cudaStreamSynchronize(stream_));
-    if (g_->tune.rounds_per_launch != rounds_per_sync_) {
+    if (g_->tune.rounds_per_launch != rounds_per_sync_ || regrid) {
       rounds_per_sync_ = g_->tune.rounds_per_launch;
       if (round_graph_) {
         cudaGraphExecDestroy(round_graph_);
@@ -836,12 +870,13 @@ class Runner {
     GraphDev gd{g_->d_beg, g_->d_adj, g_->V, g_->d_wcut};
     cudaGraph_t gr = nullptr;
     CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    cudaError_t le = cudaSuccess;
     for (uint32_t r = 0; r < rounds_per_sync_; r++) {
       k_control<<<1, 1024, 0, stream_>>>(d_qd_, d_ctl_, (int)max_slots_, d_rd_, d_pre_);
-      k_light<<<light_grid_, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, MAX_SLOTS, gd);
-      k_heavy<<<heavy_grid_, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, MAX_SLOTS, gd);
+      if (le == cudaSuccess) le = launch_light(gd, MAX_SLOTS);
+      if (le == cudaSuccess) le = launch_heavy(gd, MAX_SLOTS);
     }
-    const cudaError_t le = cudaGetLastError();
+    if (le == cudaSuccess) le = cudaGetLastError();
     const cudaError_t ce = cudaStreamEndCapture(stream_, &gr);  // always leave capture mode
     CK(le);
     CK(ce);
@@ -873,7 +908,7 @@ class Runner {
       PersistCtl* pc = d_pc_;
       void* args[] = {&d_qd_, &d_ctl_, &nsc, &d_rd_, &d_pre_, &gd, &R32, &pc};
       if (prof) CK(cudaEventRecord(ev_prof_[h][0], stream_));
-      CK(cudaLaunchCooperativeKernel((const void*)k_rounds, dim3(rounds_grid_), dim3(256), args, 0, stream_));
+      CK(cudaLaunchCooperativeKernel(kr_, dim3(rounds_grid_), dim3(threads_), args, 0, stream_));
       if (prof) CK(cudaEventRecord(ev_prof_[h][1], stream_));
       CK(cudaMemcpyAsync(h_pc_ + 2 + h, d_pc_, sizeof(PersistCtl), cudaMemcpyDeviceToHost, stream_));
       const int ns = (int)nslots_hi_;
@@ -895,9 +930,9 @@ class Runner {
       for (uint32_t r = 0; r < R; r++) {
         k_control<<<1, 1024, 0, stream_>>>(d_qd_, d_ctl_, ns, d_rd_, d_pre_);
         if (prof) CK(cudaEventRecord(pe[3 * r], stream_));
-        k_light<<<light_grid_, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
+        CK(launch_light(gd, ns));
         if (prof) CK(cudaEventRecord(pe[3 * r + 1], stream_));
-        k_heavy<<<heavy_grid_, 256, 0, stream_>>>(d_qd_, d_rd_, d_pre_, ns, gd);
+        CK(launch_heavy(gd, ns));
         if (prof) CK(cudaEventRecord(pe[3 * r + 2], stream_));
         if (prof && h_rdtrace_)  // the round's work counts, for the per-round trace
           CK(cudaMemcpyAsync(h_rdtrace_ + (size_t)h * 64 + r, d_rd_, sizeof(RoundDesc), cudaMemcpyDeviceToHost,
@@ -1060,6 +1095,10 @@ class Runner {
   uint32_t cap_num_ = 1, cap_den_ = 2, rounds_per_sync_ = 6;
   cudaEvent_t ev_[2] = {};
   unsigned light_grid_ = 148 * 4, heavy_grid_ = 148 * 2, resident_light_warps_ = 148 * 4 * 8;
+  uint32_t threads_ = 256;  // threads per block of the round kernels
+  const void* kl_ = nullptr;
+  const void* kh_ = nullptr;
+  const void* kr_ = nullptr;
   double last_call_ms_ = 0;
   double trace_ms_ = 0;
   cudaGraphExec_t round_graph_ = nullptr;
@@ -1198,6 +1237,7 @@ gst_status gst_graph_create(const uint32_t* beg_pos, const uint32_t* csr, const 
   g->tune.dp_wmax = floor_pow2(std::min(32u, std::max(1u, env_u32("GSTB_DP_WMAX", 32))));
   g->tune.sssp_wmax = floor_pow2(std::min(32u, std::max(4u, env_u32("GSTB_SSSP_WMAX", 32))));
   g->tune.merge_stage = env_u32("GSTB_MERGE_STAGE", 14);
+  g->tune.block_threads = env_u32("GSTB_BLOCK_THREADS", 256) == 128 ? 128u : 256u;
   cudaGetDevice(&g->device);
   cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device);
   {
@@ -1327,7 +1367,8 @@ gst_status gst_tuning_set(gst_graph* g, const gst_tuning* t) {
   auto pow2_in = [](uint32_t x, uint32_t lo, uint32_t hi) { return x >= lo && x <= hi && (x & (x - 1)) == 0; };
   if (!g || !t || t->delta_sssp < 1 || t->delta_dp < 1 || t->hub_min_deg < 32 || t->cap_pct < 1 ||
       t->cap_pct > 100 || t->persistent > 1 || t->rounds_per_launch < 1 || t->rounds_per_launch > 64 ||
-      !pow2_in(t->dp_wmax, 1, 32) || !pow2_in(t->sssp_wmax, 4, 32))
+      !pow2_in(t->dp_wmax, 1, 32) || !pow2_in(t->sssp_wmax, 4, 32) ||
+      (t->block_threads != 128 && t->block_threads != 256))
     return GST_BAD_INPUT;
   std::lock_guard<std::mutex> lock(g->mu);
   g->tune = *t;
@@ -1502,6 +1543,7 @@ gst_status gst_autotune(gst_graph* g, int n, const uint32_t* groups, const int32
       {&gst_tuning::dp_wmax, {4, 8, 16, 32}},
       {&gst_tuning::sssp_wmax, {8, 16, 32}},
       {&gst_tuning::merge_stage, {0, 6, 14, 30}},
+      {&gst_tuning::block_threads, {128, 256}},
   };
   for (const Cand& cd : cands) {
     for (uint32_t v : cd.vals) {
@@ -1921,8 +1963,10 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   CK(cudaMemsetAsync(q.dflag, 0, L.qbuf - L.dflag, 0));
   // grids: every SM filled to the occupancy limit of each kernel
   int bl = 0, bh = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, k_light, 256, 0));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bh, k_heavy, 256, 0));
+  const void* kl = light_kernel(256);
+  const void* kh = heavy_kernel(256);
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, kl, 256, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bh, kh, 256, 0));
   const unsigned light_grid = (unsigned)g->num_sms * (unsigned)std::max(1, bl);
   const unsigned heavy_grid = (unsigned)g->num_sms * (unsigned)std::max(1, bh);
   {
@@ -1962,8 +2006,12 @@ extern "C" gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, in
   for (;;) {
     for (uint32_t r = 0; r < R; r++) {
       k_control<<<1, 1024, 0, 0>>>(d_qd, d_ctl, 1, d_rd, d_pre);
-      k_light<<<light_grid, 256, 0, 0>>>(d_qd, d_rd, d_pre, 1, gd);
-      k_heavy<<<heavy_grid, 256, 0, 0>>>(d_qd, d_rd, d_pre, 1, gd);
+      {
+        int one = 1;
+        void* args[] = {&d_qd, &d_rd, &d_pre, &one, &gd};
+        CK(cudaLaunchKernel(kl, dim3(light_grid), dim3(256), args, 0, 0));
+        CK(cudaLaunchKernel(kh, dim3(heavy_grid), dim3(256), args, 0, 0));
+      }
     }
     CK(cudaGetLastError());
     g->launches += 3ull * R;

@@ -1882,12 +1882,15 @@ __device__ __forceinline__ void chunk_task(const QDev* qd, const RoundDesc* rd, 
     hub_chunk(qd, it, g, lane, hub, ws, wb);
 }
 
-// Light round kernel: the round's light tasks.
+// Light round kernel: the round's light tasks.  NW warps per block (4 or
+// 8); the occupancy bound keeps 24 warps per SM at 80 registers.
 #ifndef GSTB_LIGHT_MIN_BLOCKS
-#define GSTB_LIGHT_MIN_BLOCKS 3
+#define GSTB_LIGHT_MIN_BLOCKS 3  // blocks of 8 warps
 #endif
-__global__ void __launch_bounds__(256, GSTB_LIGHT_MIN_BLOCKS) k_light(const QDev* __restrict__ qd, RoundDesc* __restrict__ rd,
-                                                  const uint32_t* __restrict__ pre, int nslots, GraphDev g) {
+template <int NW>
+__global__ void __launch_bounds__(NW * 32, GSTB_LIGHT_MIN_BLOCKS * 8 / NW)
+    k_light(const QDev* __restrict__ qd, RoundDesc* __restrict__ rd, const uint32_t* __restrict__ pre, int nslots,
+            GraphDev g) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1895,9 +1898,9 @@ __global__ void __launch_bounds__(256, GSTB_LIGHT_MIN_BLOCKS) k_light(const QDev
   nslots = min(nslots, (int)__ldcg(&rd->nslots));
   // prefixes over slots of the item types with many items, staged once per block
   __shared__ uint32_t s_pre[MAX_SLOTS + 1], s_dp[MAX_SLOTS + 1], s_hop[MAX_SLOTS + 1];
-  __shared__ WarpScratch s_sc[8];
-  __shared__ WarpStat s_ws[8];
-  __shared__ WarpBuf s_wb[8];
+  __shared__ WarpScratch s_sc[NW];
+  __shared__ WarpStat s_ws[NW];
+  __shared__ WarpBuf s_wb[NW];
   WarpStat& ws = s_ws[threadIdx.x >> 5];
   WarpBuf& wb = s_wb[threadIdx.x >> 5];
   if (lane == 0) {
@@ -1922,8 +1925,10 @@ __global__ void __launch_bounds__(256, GSTB_LIGHT_MIN_BLOCKS) k_light(const QDev
 
 // Heavy round kernel: the arc chunks k_light handed over this round, then
 // bound-table rows and snapshot rows.
-__global__ void __launch_bounds__(256, 3) k_heavy(const QDev* __restrict__ qd, RoundDesc* __restrict__ rd,
-                                               const uint32_t* __restrict__ pre, int nslots, GraphDev g) {
+template <int NW>
+__global__ void __launch_bounds__(NW * 32, 24 / NW)
+    k_heavy(const QDev* __restrict__ qd, RoundDesc* __restrict__ rd, const uint32_t* __restrict__ pre, int nslots,
+            GraphDev g) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1931,10 +1936,10 @@ __global__ void __launch_bounds__(256, 3) k_heavy(const QDev* __restrict__ qd, R
   const uint32_t ntasks = __ldcg(&rd->heavy_tasks) + nbig;
   nslots = min(nslots, (int)__ldcg(&rd->nslots));
   __shared__ uint32_t s_lb[MAX_SLOTS + 1];
-  __shared__ RelaxHdr s_hub[8];
-  __shared__ uint32_t s_dl[8][KMAX][32];  // bound rows: each lane's capped distances
-  __shared__ WarpStat s_ws[8];
-  __shared__ WarpBuf s_wb[8];
+  __shared__ RelaxHdr s_hub[NW];
+  __shared__ uint32_t s_dl[NW][KMAX][32];  // bound rows: each lane's capped distances
+  __shared__ WarpStat s_ws[NW];
+  __shared__ WarpBuf s_wb[NW];
   WarpStat& ws = s_ws[threadIdx.x >> 5];
   WarpBuf& wb = s_wb[threadIdx.x >> 5];
   if (lane == 0) {
@@ -2018,18 +2023,21 @@ __device__ __forceinline__ void publish(PersistCtl* pc, uint32_t e) {
   if (!pc->hold) st_release_gpu(&pc->epoch, e);
 }
 
+template <int NW>
 struct RoundSmem {
   uint32_t pre_sssp[MAX_SLOTS + 1], pre_dp[MAX_SLOTS + 1], pre_hop[MAX_SLOTS + 1], pre_lb[MAX_SLOTS + 1];
-  WarpScratch w[8];
-  WarpStat ws[8];
-  WarpBuf wb[8];
+  WarpScratch w[NW];
+  WarpStat ws[NW];
+  WarpBuf wb[NW];
   CtlSmem ctl;
   uint32_t ok, last;
 };
 
-__global__ void __launch_bounds__(256, 3) k_rounds(QDev* qd, QCtl* ctl, int nslots_ctl, RoundDesc* rd, uint32_t* pre,
-                                                GraphDev g, uint32_t R, PersistCtl* pc) {
-  __shared__ RoundSmem sm;
+template <int NW>
+__global__ void __launch_bounds__(NW * 32, 24 / NW)
+    k_rounds(QDev* qd, QCtl* ctl, int nslots_ctl, RoundDesc* rd, uint32_t* pre, GraphDev g, uint32_t R,
+             PersistCtl* pc) {
+  __shared__ RoundSmem<NW> sm;
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
   const uint32_t warp = blockIdx.x * (blockDim.x >> 5) + wib;
   const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
@@ -2110,6 +2118,19 @@ __global__ void __launch_bounds__(256, 3) k_rounds(QDev* qd, QCtl* ctl, int nslo
     }
     __syncthreads();  // sm.ok and sm.last are rewritten next round
   }
+}
+
+// Host side: the round kernels of one block size, 128 or 256 threads (null
+// for any other; 512-thread blocks would need more than the 48 KB of static
+// shared memory a block can hold: each warp stages its appends in 2 KB).
+const void* light_kernel(int threads) {
+  return threads == 128 ? (const void*)k_light<4> : threads == 256 ? (const void*)k_light<8> : nullptr;
+}
+const void* heavy_kernel(int threads) {
+  return threads == 128 ? (const void*)k_heavy<4> : threads == 256 ? (const void*)k_heavy<8> : nullptr;
+}
+const void* rounds_kernel(int threads) {
+  return threads == 128 ? (const void*)k_rounds<4> : threads == 256 ? (const void*)k_rounds<8> : nullptr;
 }
 
 }  // namespace gstb

@@ -46,7 +46,7 @@ class GstError(RuntimeError):
 
 
 TUNING_FIELDS = ("delta_sssp", "delta_dp", "hub_min_deg", "cap_pct", "persistent", "rounds_per_launch",
-                 "dp_wmax", "sssp_wmax", "merge_stage")
+                 "dp_wmax", "sssp_wmax", "merge_stage", "block_threads")
 
 
 class _Tuning(ctypes.Structure):

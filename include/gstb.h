@@ -165,7 +165,8 @@ gst_status gst_query_noalloc(gst_graph* g, const uint32_t* groups, int k, int D,
  * and GPUGST+/include/util.h:19-33).  Defaults, overridable at
  * gst_graph_create by GSTB_DELTA_SSSP / GSTB_DELTA_DP / GSTB_HUB_MIN_DEG /
  * GSTB_SSSP_CAP_PCT / GSTB_PERSIST / GSTB_ROUNDS_PER_SYNC / GSTB_DP_WMAX /
- * GSTB_SSSP_WMAX / GSTB_MERGE_STAGE: 16, 8, 256, 60, 0, 4, 32, 32, 14.  None
+ * GSTB_SSSP_WMAX / GSTB_MERGE_STAGE / GSTB_BLOCK_THREADS: 16, 8, 256, 60, 0,
+ * 4, 32, 32, 14, 256.  None
  * of them changes a result, only the work schedule and how tight the lower
  * bounds are. */
 typedef struct gst_tuning {
@@ -182,6 +183,8 @@ typedef struct gst_tuning {
   uint32_t sssp_wmax;    /* most distance items (vertices) per warp task: 4, 8, 16 or 32 */
   uint32_t merge_stage;  /* merge tile: a DP state with at least this many merge partners first
                             stages its vertex's table and bound rows in shared memory (0: never) */
+  uint32_t block_threads; /* threads per block of the round kernels: 128 or 256 (24 warps per SM
+                             either way) */
 } gst_tuning;
 
 gst_status gst_tuning_get(gst_graph* g, gst_tuning* out);
@@ -190,7 +193,8 @@ gst_status gst_tuning_set(gst_graph* g, const gst_tuning* t);
  * (laid out as for gst_query_batch) under candidate settings (cap_pct 50/60/
  * 67/75, delta_sssp 8..64, delta_dp 2..16, hub_min_deg 128..1024, persistent
  * 0/1, rounds_per_launch 2..16, dp_wmax 4..32, sssp_wmax 8..32, merge_stage
- * 0/6/14/30), one parameter at a time, and keeps the fastest.  objective 0 = batch throughput
+ * 0/6/14/30, block_threads 128/256), one parameter at a time, and keeps the
+ * fastest.  objective 0 = batch throughput
  * (gst_query_batch), 1 = one query at a time (gst_query).  The chosen
  * settings stay on the graph; out (may be null) receives them. */
 gst_status gst_autotune(gst_graph* g, int n, const uint32_t* groups, const int32_t* ks, const int32_t* Ds,

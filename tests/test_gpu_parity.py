@@ -234,13 +234,15 @@ def test_autotune_keeps_results_exact(gst_lib, oracle_mod, c1):
     assert t["hub_min_deg"] in (128, 256, 512, 1024) and t["cap_pct"] in (50, 60, 67, 75)
     assert t["persistent"] in (0, 1) and t["rounds_per_launch"] in (2, 4, 8, 16)
     assert t["dp_wmax"] in (4, 8, 16, 32) and t["sssp_wmax"] in (8, 16, 32) and t["merge_stage"] in (0, 6, 14, 30)
+    assert t["block_threads"] in (128, 256)
     assert E.tuning() == t
     res = E.query_batch(list(qs[3][16:28]))
     for q, r in zip(qs[3][16:28], res):
         assert r.status == eng.GST_OK and r.cost == O.prunedpp(g, gr, q, 0).cost
     for persistent in (0, 1):
         want = {"delta_sssp": 8, "delta_dp": 2, "hub_min_deg": 128, "cap_pct": 100, "persistent": persistent,
-                "rounds_per_launch": 2, "dp_wmax": 4, "sssp_wmax": 8, "merge_stage": 6 * persistent}
+                "rounds_per_launch": 2, "dp_wmax": 4, "sssp_wmax": 8, "merge_stage": 6 * persistent,
+                "block_threads": 256 - 128 * persistent}
         E.set_tuning(**want)
         assert E.tuning() == want
         for q in qs[3][28:32]:
@@ -248,6 +250,8 @@ def test_autotune_keeps_results_exact(gst_lib, oracle_mod, c1):
             assert r.status == eng.GST_OK and r.cost == O.prunedpp(g, gr, q, 0).cost
     with pytest.raises(eng.GstError):
         E.set_tuning(dp_wmax=3)  # not a power of two
+    with pytest.raises(eng.GstError):
+        E.set_tuning(block_threads=512)
     with pytest.raises(ValueError):
         E.set_tuning(block=1)
     E.close()

@@ -1,7 +1,8 @@
 """The persistent round launch (k_rounds: a block of rounds as one cooperative
 launch) against the CUDA-graph round blocks (control / light / heavy launches
-per round) and the oracle, and its bounded waits: a launch whose control steps
-are held ends with GST_DEVICE_TIMEOUT and the device stays usable."""
+per round) and the oracle, at both block sizes, and its bounded waits: a
+launch whose control steps are held ends with GST_DEVICE_TIMEOUT and the
+device stays usable."""
 import time
 
 import pytest
@@ -29,16 +30,17 @@ def test_persistent_matches_graph_rounds_and_oracle(gst_lib, oracle_mod, c1):
     queries, Ds = _mixed(qs)
     E = eng.Engine.from_instance(g, gr)
     got = {}
-    for mode in (0, 1):
-        for rpl in (1, 4, 16):
-            E.set_tuning(persistent=mode, rounds_per_launch=rpl)
-            batch = E.query_batch(queries, Ds)
-            plain = [E.query(q, D=d) for q, d in zip(queries[8:12], Ds[8:12])]
-            got[(mode, rpl)] = [(r.status, r.cost) for r in batch] + [(r.status, r.cost) for r in plain]
-            for q, d, r in zip(queries, Ds, batch):
-                if r.status == eng.GST_OK:
-                    assert not O.validate(g, gr, q, d, r.cost, r.root, r.edges)
-    ref = got[(0, 4)]
+    # launch mode x rounds per launch at 256 threads a block, and both modes at 128
+    configs = [(m, r, 256) for m in (0, 1) for r in (1, 4, 16)] + [(0, 4, 128), (1, 4, 128)]
+    for mode, rpl, bt in configs:
+        E.set_tuning(persistent=mode, rounds_per_launch=rpl, block_threads=bt)
+        batch = E.query_batch(queries, Ds)
+        plain = [E.query(q, D=d) for q, d in zip(queries[8:12], Ds[8:12])]
+        got[(mode, rpl, bt)] = [(r.status, r.cost) for r in batch] + [(r.status, r.cost) for r in plain]
+        for q, d, r in zip(queries, Ds, batch):
+            if r.status == eng.GST_OK:
+                assert not O.validate(g, gr, q, d, r.cost, r.root, r.edges)
+    ref = got[(0, 4, 256)]
     for key, val in got.items():
         assert val == ref, key
     for (st, cost), q, d in zip(ref, queries, Ds):
