@@ -65,6 +65,10 @@ struct RoundDesc {
   uint32_t hub_min_rest;  // ... and only when at least this many arcs remain under the limit
   uint32_t hub_max_items; // chunk only in rounds with fewer distance items (latency-bound rounds)
   uint32_t hub_on;        // set by k_control for the current round
+  // larger rounds: items of at least hub_big_deg arcs are still chunked in
+  // rounds with fewer than hub_max_items2 distance items (0: never)
+  uint32_t hub_max_items2, hub_big_deg;
+  uint32_t hub_deg;       // this round's chunking threshold for distance items (INF32: none; k_control)
   uint32_t grow_chunks;   // DP grows hand hub arcs out this round (set by k_control)
   uint32_t sssp_w;        // distance items per warp task this round (set by k_control)
   uint32_t dp_w;          // DP states per warp task this round (set by k_control)

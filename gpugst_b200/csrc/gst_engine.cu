@@ -442,6 +442,8 @@ class Runner {
       rd.hub_min_deg = g_->tune.hub_min_deg;
       rd.hub_min_rest = env_u32("GSTB_HUB_MIN_REST", 128);
       rd.hub_max_items = env_u32("GSTB_HUB_MAX_ITEMS", 1000000);
+      rd.hub_max_items2 = env_u32("GSTB_HUB_MAX_ITEMS2", 8000000);
+      rd.hub_big_deg = std::max(32u, env_u32("GSTB_HUB_BIG_DEG", 1024));
       // task widths are sized for the warps resident at once
       rd.light_warps = light_warps();
       rd.sssp_w = 4;

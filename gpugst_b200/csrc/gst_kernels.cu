@@ -940,7 +940,7 @@ __device__ void sssp_task(const QDev* qd, const uint32_t* __restrict__ pre, int 
       n = a1 - b0;
       // hub: hand all but the first HUB_LOCAL arcs to k_heavy in chunks of
       // HUB_CHUNK arcs, one warp each
-      if (rd->hub_on && n >= rd->hub_min_deg && n - HUB_LOCAL >= rd->hub_min_rest) {
+      if (n >= rd->hub_deg && n - HUB_LOCAL >= rd->hub_min_rest) {
         const uint32_t st0 = b0 + HUB_LOCAL;
         const uint32_t nch = (a1 - st0 + HUB_CHUNK - 1u) / HUB_CHUNK;
         const uint32_t cb = atomicAdd(&rd->n_big, nch);
@@ -1765,8 +1765,13 @@ __device__ void control_step(QDev* qd, QCtl* ctl, int nslots, RoundDesc* rd, uin
     rd->next_light = 0;
     rd->next_heavy = 0;
     // hub chunking pays off only when the round is too small to fill the GPU
-    rd->hub_on =
-        (rd->big != nullptr && rd->items[T_SSSP] + rd->items[T_DP] + rd->items[T_HOP] < rd->hub_max_items) ? 1u : 0u;
+    const uint32_t n_items = rd->items[T_SSSP] + rd->items[T_DP] + rd->items[T_HOP];
+    rd->hub_on = (rd->big != nullptr && n_items < rd->hub_max_items) ? 1u : 0u;
+    // distance items: every hub in small rounds; in larger ones (a single
+    // query's dense rounds) only the biggest hubs, whose one warp would
+    // otherwise finish long after the rest
+    rd->hub_deg = rd->hub_on ? rd->hub_min_deg
+                             : ((rd->big != nullptr && n_items < rd->hub_max_items2) ? rd->hub_big_deg : INF32);
     // DP tasks that hold several states hand their hub grows out in every
     // round: a task with a few hub states would otherwise grow them one
     // after another on one warp
@@ -2083,7 +2088,7 @@ __global__ void __launch_bounds__(NW * 32, 24 / NW)
     // phase 1 done in this block: its chunk entries are written.  Rounds
     // that hand out no chunks (every block reads the same flags) skip the
     // grid-wide wait for the others
-    if (rd->big != nullptr && (__ldcg(&rd->hub_on) | __ldcg(&rd->grow_chunks))) {
+    if (rd->big != nullptr && (__ldcg(&rd->hub_deg) != INF32 || __ldcg(&rd->grow_chunks) != 0u)) {
       p1++;
       __syncthreads();
       if (threadIdx.x == 0) {
