@@ -625,9 +625,22 @@ def main():
             qps, lats, _ = closed_loop(engine, E, reqs2, inflight)
             sw2.append({"inflight": inflight, "qps": qps, "p50_ms": pct(lats, 50), "p99_ms": pct(lats, 99),
                         "vs_plain": qps / p_qps, "queries": len(reqs2)})
+        # round kernels' roofline on this workload (profiled 90-query batch)
+        E.profile(True)
+        E.profile_reset()
+        q2, D2 = qs2[100:190], Ds2[100:190]
+        E.query_batch(q2, D2)
+        lm2, hm2, r2, st2 = E.profile_read()
+        E.profile(False)
+        lb2 = sum(g2.V * (32 + 2 * (1 << len(q))) for q in q2)
+        bytes2 = distance_work_bytes(st2) + dp_work_bytes(st2, lb2)
+        ach2 = bytes2 / ((lm2 + hm2) / 1e3) / 1e9 if lm2 + hm2 > 0 else 0.0
         c2 = {"workload": workload_desc("c2"), "plain_qps": p_qps, "plain_p50_ms": pct(pl, 50),
               "plain_p99_ms": pct(pl, 99), "batched_qps_e2e": b_qps, "batched_vs_plain_e2e": b_qps / p_qps,
-              "batched_device_ms": rb[0].device_ms, "serve_sweep": sw2}
+              "batched_device_ms": rb[0].device_ms, "serve_sweep": sw2,
+              "roofline": {"bound": "hbm", "kernel": "round (k_light + k_heavy)", "achieved": ach2, "peak": peak,
+                           "unit": "GB/s", "frac": ach2 / peak, "peak_kind": peak_kind, "rounds": r2,
+                           "kernel_ms": {"k_light": lm2, "k_heavy": hm2}, "algorithmic_bytes": bytes2}}
 
     if rank == 0:
         best_pt = max(sweep, key=lambda x: x["qps"]) if sweep else None
