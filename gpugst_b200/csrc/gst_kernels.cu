@@ -773,7 +773,7 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
 
   for (uint32_t base = f0; base < f1; base += 32u * SSSP_U) {
     uint2 arc[SSSP_U];
-    uint32_t itm[SSSP_U];
+    uint32_t itm[SSSP_U], lim[SSSP_U];
     bool ok[SSSP_U];
 #pragma unroll
     for (int u = 0; u < SSSP_U; u++) {
@@ -791,12 +791,15 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
       const uint32_t start = pos == 0u ? 0u : xs;
       ok[u] = f < f1;
       itm[u] = ok[u] ? pos : i0;
-      arc[u] = ok[u] ? __ldg(g.adj + h[itm[u]].a0 + (f - start)) : make_uint2(0u, 0u);
+      // the item's weight limit and first arc in one 8-byte shared load
+      const uint2 la = *reinterpret_cast<const uint2*>(&h[itm[u]].lim);
+      lim[u] = la.x;
+      arc[u] = ok[u] ? __ldg(g.adj + la.y + (f - start)) : make_uint2(0u, 0u);
     }
     uint4 ra[SSSP_U], rb[SSSP_U];
 #pragma unroll
     for (int u = 0; u < SSSP_U; u++) {
-      ok[u] = ok[u] && arc[u].y <= h[itm[u]].lim;
+      ok[u] = ok[u] && arc[u].y <= lim[u];
       if (ok[u]) {
         const uint4* row = reinterpret_cast<const uint4*>(dist + (size_t)arc[u].x * 8);
         ra[u] = __ldcg(row);
@@ -811,13 +814,16 @@ __device__ __forceinline__ void relax_flat(const QDev& q, const RelaxHdr* __rest
       nn[u] = nf[u] = 0u;
       if (ok[u]) {
         cnt.arcs++;
-        const RelaxHdr& hh = h[itm[u]];
-        const uint32_t rm = hh.rm;
+        // the item's distances and group mask in two 16-byte shared loads
+        const uint4* hv = reinterpret_cast<const uint4*>(&h[itm[u]]);
+        const uint4 h0 = hv[0], h1 = hv[1];
+        const uint32_t rm = h1.w;
+        const uint32_t dv[KMAX] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z};
         const uint32_t du[KMAX] = {ra[u].x, ra[u].y, ra[u].z, ra[u].w, rb[u].x, rb[u].y, rb[u].z};
 #pragma unroll
         for (int t = 0; t < KMAX; t++) {
           if ((rm >> t) & 1u) {
-            const uint32_t dt = hh.d[t];
+            const uint32_t dt = dv[t];
             const uint32_t nd = dt + arc[u].y;
             if (nd >= dt && nd <= capb && nd < du[t]) {
               red_min(dist + (size_t)arc[u].x * ROW + t, nd);
