@@ -207,11 +207,14 @@ class Arena {
     n = align_up(std::max<size_t>(n, 1), 256);
     auto it = by_size_.lower_bound(n);
     if (it == by_size_.end()) {
-      // A growth of this size already failed and nothing has been freed
-      // since: waiting for running queries is cheaper than another failing
-      // cudaMalloc (and its trim) on every admission attempt, which stalled
-      // the host while the GPU ran out of launched rounds.
-      if (n >= grow_failed_) return nullptr;
+      // A growth of this size already failed and no memory went back to the
+      // device since (a workspace freed inside the arena gives it none):
+      // while this arena's queries run, waiting for their blocks to coalesce
+      // is cheaper than another failing cudaMalloc on every admission
+      // attempt, which held the host for up to 130 ms each time while the GPU
+      // ran out of launched rounds.  With nothing in use, growth is retried
+      // (with a trim), so a request never waits on itself.
+      if (n >= grow_failed_ && in_use_ != 0) return nullptr;
       if (!grow(n)) {
         grow_failed_ = n;
         return nullptr;
@@ -237,7 +240,6 @@ class Arena {
     size_t n = u->second;
     used_.erase(u);
     in_use_ -= n;
-    grow_failed_ = SIZE_MAX;  // a larger block may fit now
     const char* base = chunk_base(p);
     // merge with the free neighbours inside the same chunk
     auto nx = free_.find(p + n);
@@ -353,7 +355,7 @@ class Arena {
   std::multimap<size_t, char*> by_size_;  // size -> free block
   std::unordered_map<char*, size_t> used_;
   size_t held_ = 0, in_use_ = 0, free_total_ = 0;
-  size_t grow_failed_ = SIZE_MAX;  // smallest growth that failed since the last free
+  size_t grow_failed_ = SIZE_MAX;  // smallest growth that failed since memory last went back to the device
   std::atomic<int>* fail_ = nullptr;
 };
 
