@@ -587,9 +587,12 @@ def main():
     plain_dev_qps = len(plain_dev) / (sum(plain_dev) / 1e3) if plain_dev else None
 
     # closed-loop serving at several concurrencies (the latency / throughput trade-off)
+    # (each point runs at least 8 x its concurrency requests, so that the
+    # ramp-up and the drain do not dominate its rate)
     sweep = []
-    reqs = [(qs[(rank * 104729 + 7 * i) % nq_set], Ds[(rank * 104729 + 7 * i) % nq_set]) for i in range(n_sweep)]
     for inflight in [int(x) for x in args.sweep.split(",") if x]:
+        nreq = n_sweep if args.sweep_queries else max(n_sweep, 8 * inflight)
+        reqs = [(qs[(rank * 104729 + 7 * i) % nq_set], Ds[(rank * 104729 + 7 * i) % nq_set]) for i in range(nreq)]
         qps, lats, sts = closed_loop(engine, E, reqs, inflight)
         sweep.append({"inflight": inflight, "qps": qps, "p50_ms": pct(lats, 50), "p99_ms": pct(lats, 99),
                       "vs_plain": qps / plain_qps if plain_qps else None, "queries": len(reqs)})
