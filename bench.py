@@ -419,7 +419,7 @@ def main():
     ap.add_argument("--workload", default="c4", choices=["c4", "c4s", "c2", "c1"])
     ap.add_argument("--batch", type=int, default=0, help="queries per step (default: 128 on c4, 90 on c2)")
     ap.add_argument("--plain", type=int, default=300, help="queries on the plain per-query path")
-    ap.add_argument("--sweep", default="1,2,4,8,16,32", help="closed-loop serving concurrencies")
+    ap.add_argument("--sweep", default="1,2,4,8,16,32,64", help="closed-loop serving concurrencies")
     ap.add_argument("--sweep-queries", type=int, default=0, help="queries per sweep point (default 64 on c4)")
     ap.add_argument("--c5-rates", default="50,200,1000", help="open-loop Poisson rates (c4 only)")
     ap.add_argument("--c5-seconds", type=float, default=10.0, help="arrival window per rate")
