@@ -68,6 +68,9 @@ struct RoundDesc {
   // larger rounds: items of at least hub_big_deg arcs are still chunked in
   // rounds with fewer than hub_max_items2 distance items (0: never)
   uint32_t hub_max_items2, hub_big_deg;
+  // ... and only when they exceed 1/hub_share_div of a warp's share of the
+  // round's arcs (items x avg_deg / light_warps; 0: no such test)
+  uint32_t hub_share_div, avg_deg;
   uint32_t hub_deg;       // this round's chunking threshold for distance items (INF32: none; k_control)
   uint32_t grow_chunks;   // DP grows hand hub arcs out this round (set by k_control)
   uint32_t sssp_w;        // distance items per warp task this round (set by k_control)
@@ -96,7 +99,10 @@ struct PersistCtl {
   uint32_t pad;
   unsigned long long timeout_ns;  // limit of every wait
 };
-constexpr uint32_t HUB_CHUNK = 256;     // arcs per chunk (one warp)
+#ifndef GSTB_HUB_CHUNK
+#define GSTB_HUB_CHUNK 256
+#endif
+constexpr uint32_t HUB_CHUNK = GSTB_HUB_CHUNK;  // arcs per chunk (one warp)
 constexpr uint32_t LB_CHUNK = 1u << 22; // bound-table rows (vertices) per query per round
 
 enum Phase : int32_t {

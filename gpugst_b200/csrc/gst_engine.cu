@@ -446,6 +446,8 @@ class Runner {
       rd.hub_max_items = env_u32("GSTB_HUB_MAX_ITEMS", 1000000);
       rd.hub_max_items2 = env_u32("GSTB_HUB_MAX_ITEMS2", 8000000);
       rd.hub_big_deg = std::max(32u, env_u32("GSTB_HUB_BIG_DEG", 1024));
+      rd.hub_share_div = env_u32("GSTB_HUB_SHARE_DIV", 16);
+      rd.avg_deg = (uint32_t)std::max<uint64_t>(1, (g_->arcs + g_->V - 1) / std::max<uint32_t>(1, g_->V));
       // task widths are sized for the warps resident at once
       rd.light_warps = light_warps();
       rd.sssp_w = 4;

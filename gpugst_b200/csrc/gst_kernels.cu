@@ -1775,9 +1775,16 @@ __device__ void control_step(QDev* qd, QCtl* ctl, int nslots, RoundDesc* rd, uin
     rd->hub_on = (rd->big != nullptr && n_items < rd->hub_max_items) ? 1u : 0u;
     // distance items: every hub in small rounds; in larger ones (a single
     // query's dense rounds) only the biggest hubs, whose one warp would
-    // otherwise finish long after the rest
+    // otherwise finish long after the rest: at least hub_big_deg arcs and
+    // more than 1/hub_share_div of a warp's share of the round's arcs
+    uint32_t big_deg = rd->hub_big_deg;
+    if (rd->hub_share_div != 0u) {
+      const unsigned long long share =
+          (unsigned long long)n_items * rd->avg_deg / max(1u, rd->light_warps) / rd->hub_share_div;
+      big_deg = (uint32_t)max((unsigned long long)big_deg, min(share, (unsigned long long)INF32 - 1ull));
+    }
     rd->hub_deg = rd->hub_on ? rd->hub_min_deg
-                             : ((rd->big != nullptr && n_items < rd->hub_max_items2) ? rd->hub_big_deg : INF32);
+                             : ((rd->big != nullptr && n_items < rd->hub_max_items2) ? big_deg : INF32);
     // DP tasks that hold several states hand their hub grows out in every
     // round: a task with a few hub states would otherwise grow them one
     // after another on one warp
