@@ -224,9 +224,11 @@ gst_status gst_query_batch_ratio(gst_graph* g, int n, const uint32_t* groups, co
 typedef struct gst_server gst_server;
 
 /* hbm_budget_bytes: device bytes the admitted queries' workspaces may hold
- * at once (0 = 80% of the free memory at open); max_inflight: queries on the
- * device at once (0 = up to 1023).  Each result's latency_ms is the time from
- * submission to completion. */
+ * at once (0 = 80% of the free memory at open), reserved in one allocation
+ * at open (GSTB_SERVE_RESERVE_MB caps the reservation; beyond it the loop
+ * allocates as requests need); max_inflight: queries on the device at once
+ * (0 = up to 1023).  Each result's latency_ms is the time from submission to
+ * completion. */
 gst_status gst_serve_open(gst_graph* g, uint64_t hbm_budget_bytes, int max_inflight,
                           gst_server** out);
 /* Never blocks.  Copies the groups.  GST_BUSY if the pending queue is full. */
